@@ -1,0 +1,79 @@
+"""In-tree build of libaospectrum_b200.so for sm_100a with nvcc.
+
+``python -m aospectrum_b200.build`` compiles every ``csrc/*.cu`` into one
+shared library next to this file.  Sources are compiled in parallel into
+``_build/`` and relinked only when a source or header changed.
+"""
+
+from __future__ import annotations
+
+import concurrent.futures
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+INCLUDE = HERE.parent / "include"
+BUILD = HERE.parent / "_build"
+LIBRARY = HERE / "libaospectrum_b200.so"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+         "--expt-relaxed-constexpr", "-I", str(INCLUDE), "-I", str(CSRC)]
+
+
+def _nvcc() -> str:
+    found = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(found).exists():
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build")
+    return found
+
+
+def _cutlass_include() -> list[str]:
+    import site
+
+    for root in site.getsitepackages():
+        cand = Path(root) / "flashinfer" / "data" / "cutlass" / "include"
+        if (cand / "cute" / "arch" / "mma_sm100_desc.hpp").exists():
+            return ["-I", str(cand)]
+    return []
+
+
+def build(verbose: bool = False, jobs: int | None = None) -> Path:
+    nvcc = _nvcc()
+    BUILD.mkdir(exist_ok=True)
+    sources = sorted(CSRC.glob("*.cu"))
+    headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    newest_header = max((h.stat().st_mtime for h in headers), default=0.0)
+    extra = _cutlass_include()
+
+    def compile_one(src: Path) -> Path:
+        obj = BUILD / (src.stem + ".o")
+        if obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, newest_header):
+            return obj
+        cmd = [nvcc, *ARCH, *FLAGS, *extra, "-c", str(src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        proc = subprocess.run(cmd, capture_output=True, text=True)
+        if proc.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src.name}:\n{proc.stdout}\n{proc.stderr}")
+        if verbose and proc.stderr.strip():
+            print(proc.stderr, flush=True)
+        return obj
+
+    workers = jobs or min(8, os.cpu_count() or 1)
+    with concurrent.futures.ThreadPoolExecutor(workers) as pool:
+        objects = list(pool.map(compile_one, sources))
+    newest_obj = max(o.stat().st_mtime for o in objects)
+    if not LIBRARY.exists() or LIBRARY.stat().st_mtime < newest_obj:
+        cmd = [nvcc, *ARCH, "-shared", "-o", str(LIBRARY), *map(str, objects), "-lcudart"]
+        proc = subprocess.run(cmd, capture_output=True, text=True)
+        if proc.returncode != 0:
+            raise RuntimeError(f"link failed:\n{proc.stdout}\n{proc.stderr}")
+    return LIBRARY
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

@@ -1,0 +1,338 @@
+// Library facts and the drop-in uniform-batch shifted solve with host
+// buffers (replaces aospectrum_cudss_solve_complex64_ubatch_v1,
+// native/src/aospectrum_cudss_complex64_ubatch.c:243-672).
+//
+// Differences from the reference call that the request/result layout hides:
+//   - the symbolic plan of the most recent CSR pattern is cached, so a run
+//     of calls on one pattern pays for the analysis once (the reference
+//     re-runs cuDSS ANALYSIS on every call);
+//   - the factorization is complex64 with FP32 tile updates and two FP64
+//     iterative-refinement steps (the reference configures two cuDSS
+//     complex64 refinement steps, aospectrum_cudss_complex64_ubatch.c:375).
+#include "plan.h"
+#include "factor.h"
+
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+namespace aosb {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+
+double now_seconds() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+uint64_t fnv1a(uint64_t h, const void* data, size_t bytes) {
+  const unsigned char* p = (const unsigned char*)data;
+  for (size_t i = 0; i < bytes; ++i) {
+    h ^= p[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+struct PlanCache {
+  std::mutex mu;
+  int device = -1;
+  int64_t n = 0, nnz = 0;
+  uint64_t hash = 0;
+  aosb_plan* plan = nullptr;
+};
+PlanCache g_cache;
+
+// column-major complex64 [b][col][row] -> row-major complex128 [b][row][col]
+__global__ void cm_to_rm_kernel(int64_t n, int L, const float2* __restrict__ src,
+                                double2* __restrict__ dst) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (idx >= n * L) return;
+  const int64_t row = idx / L, col = idx - (idx / L) * L;
+  const float2 v = src[((size_t)b * L + col) * n + row];
+  dst[(size_t)b * n * L + idx] = make_double2(v.x, v.y);
+}
+
+__global__ void rm_to_cm_kernel(int64_t n, int L, const double2* __restrict__ src,
+                                float2* __restrict__ dst) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (idx >= n * L) return;
+  const int64_t col = idx / n, row = idx - (idx / n) * n;
+  const double2 v = src[(size_t)b * n * L + row * L + col];
+  dst[(size_t)b * n * L + idx] = make_float2((float)v.x, (float)v.y);
+}
+
+__global__ void iota_kernel(int n, int32_t* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = i;
+}
+
+int pick_tile(int64_t n) {
+  if (n <= 512) return 32;
+  if (n <= 6000) return 64;
+  return 128;
+}
+
+}  // namespace
+}  // namespace aosb
+
+extern "C" {
+
+uint32_t aosb_abi_version(void) { return AOSPECTRUM_B200_ABI_VERSION; }
+
+uint64_t aosb_launch_count(void) { return aosb::g_launches.load(); }
+
+const char* aosb_build_info(void) {
+  return "aospectrum_b200 abi=1 arch=sm_100a kernels=bloch,plan,tile-lu-fp32,tile-lu-bf16x3-tcgen05,"
+         "block-solve,ir-fp64,ciss-fp64";
+}
+
+int aospectrum_b200_solve_complex64_ubatch_v1(const aospectrum_b200_ubatch_request_v1* req,
+                                              aospectrum_b200_ubatch_result_v1* res) {
+  using namespace aosb;
+  if (req == nullptr || res == nullptr) return 1;
+  std::memset(res, 0, sizeof(*res));
+  res->abi_version = AOSPECTRUM_B200_ABI_VERSION;
+  res->struct_size = (uint32_t)sizeof(*res);
+  char* em = res->error_message;
+  const size_t ec = AOSPECTRUM_B200_ERROR_CAPACITY;
+  auto fail = [&](int code) {
+    res->status = code;
+    return 1;
+  };
+  const double t0 = now_seconds();
+  if (req->abi_version != AOSPECTRUM_B200_ABI_VERSION || req->struct_size != sizeof(*req))
+    return fail(set_error(em, ec, AOSB_ERR_ABI, "request ABI mismatch"));
+  if (req->n <= 0 || req->n > INT32_MAX || req->nnz <= 0 || req->nnz > INT32_MAX)
+    return fail(set_error(em, ec, AOSB_ERR_DIMS, "matrix dimensions exceed the int32 CSR ABI"));
+  if (req->batch_count <= 0 || req->batch_count > 64 || req->rhs_count <= 0 ||
+      req->rhs_count > 256)
+    return fail(set_error(em, ec, AOSB_ERR_BATCH, "invalid uniform-batch dimensions"));
+  if (req->indptr == nullptr || req->indices == nullptr || req->values == nullptr ||
+      req->rhs == nullptr || req->solution == nullptr)
+    return fail(set_error(em, ec, AOSB_ERR_NULL, "required input or output pointer is null"));
+  const int64_t n = req->n, nnz = req->nnz;
+  const int B = req->batch_count, L = req->rhs_count;
+  if (req->indptr[0] != 0 || req->indptr[n] != nnz)
+    return fail(set_error(em, ec, AOSB_ERR_INDPTR, "CSR row offsets do not span the declared nnz"));
+  int64_t diag = 0;
+  for (int64_t r = 0; r < n; ++r) {
+    const int32_t b = req->indptr[r], e = req->indptr[r + 1];
+    if (b < 0 || e < b || e > nnz)
+      return fail(set_error(em, ec, AOSB_ERR_CSR_MONOTONIC, "CSR row offsets are not monotonic"));
+    int32_t prev = -1;
+    bool has = false;
+    for (int32_t q = b; q < e; ++q) {
+      const int32_t c = req->indices[q];
+      if (c < 0 || c >= n)
+        return fail(set_error(em, ec, AOSB_ERR_CSR_COLUMN, "CSR column index is outside the matrix"));
+      if (c <= prev)
+        return fail(set_error(em, ec, AOSB_ERR_CSR_ORDER, "CSR columns must be sorted and duplicate-free"));
+      prev = c;
+      has |= c == r;
+    }
+    diag += has;
+  }
+  if (diag != n)
+    return fail(set_error(em, ec, AOSB_ERR_DIAGONAL,
+                          "shifted matrices are missing diagonal entries: %lld/%lld",
+                          (long long)diag, (long long)n));
+  for (int64_t i = 0; i < (int64_t)B * nnz; ++i)
+    if (!std::isfinite(req->values[i].real) || !std::isfinite(req->values[i].imag))
+      return fail(set_error(em, ec, AOSB_ERR_NONFINITE_MATRIX,
+                            "shifted matrix batch contains non-finite values"));
+  for (int64_t i = 0; i < (int64_t)B * n * L; ++i)
+    if (!std::isfinite(req->rhs[i].real) || !std::isfinite(req->rhs[i].imag))
+      return fail(set_error(em, ec, AOSB_ERR_NONFINITE_RHS,
+                            "right-hand-side batch contains non-finite values"));
+  res->n = n;
+  res->nnz = nnz;
+  res->diagonal_count = diag;
+  res->batch_count = B;
+  res->rhs_count = L;
+  res->iterative_refinement_steps = 2;
+
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(set_error(em, ec, AOSB_ERR_CUDA, "no CUDA device"));
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  res->free_device_bytes_before = free_b;
+  res->total_device_bytes = total_b;
+
+  // Symbolic plan (cached per pattern).
+  const double ta = now_seconds();
+  uint64_t h = 1469598103934665603ull;
+  h = fnv1a(h, req->indptr, sizeof(int32_t) * (size_t)(n + 1));
+  h = fnv1a(h, req->indices, sizeof(int32_t) * (size_t)nnz);
+  aosb_plan* plan = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_cache.mu);
+    if (g_cache.plan != nullptr && g_cache.device == dev && g_cache.n == n &&
+        g_cache.nnz == nnz && g_cache.hash == h) {
+      plan = g_cache.plan;
+    } else {
+      if (g_cache.plan != nullptr) aosb_plan_destroy(g_cache.plan);
+      g_cache.plan = nullptr;
+      std::vector<int64_t> ip(req->indptr, req->indptr + n + 1);
+      aosb_plan_options_v1 opt{AOSPECTRUM_B200_ABI_VERSION, sizeof(aosb_plan_options_v1),
+                               pick_tile(n), 1, 4 * pick_tile(n), 1};
+      int rc = aosb_plan_create(n, ip.data(), req->indices, nullptr, 0, &opt, &plan, em, ec);
+      if (rc != 0) return fail(rc);
+      rc = aosb_plan_upload(plan, em, ec);
+      if (rc != 0) {
+        aosb_plan_destroy(plan);
+        return fail(rc);
+      }
+      g_cache.plan = plan;
+      g_cache.device = dev;
+      g_cache.n = n;
+      g_cache.nnz = nnz;
+      g_cache.hash = h;
+    }
+  }
+  res->analysis_seconds = now_seconds() - ta;
+  res->reported_factor_nnz = plan->n_slots * plan->T * plan->T;
+
+  // Device buffers.
+  const double tu = now_seconds();
+  cudaStream_t st = nullptr;
+  float2* d_vals = nullptr;
+  float2* d_rhs_cm = nullptr;
+  double2 *d_b = nullptr, *d_x = nullptr, *d_r = nullptr;
+  float2* d_work = nullptr;
+  float* d_factor = nullptr;
+  int32_t *d_piv = nullptr, *d_status = nullptr, *d_pk = nullptr;
+  double2* d_shift = nullptr;
+  int rc = 0;
+  auto cleanup = [&]() {
+    cudaFree(d_vals); cudaFree(d_rhs_cm); cudaFree(d_b); cudaFree(d_x); cudaFree(d_r);
+    cudaFree(d_work); cudaFree(d_factor); cudaFree(d_piv); cudaFree(d_status); cudaFree(d_pk);
+    cudaFree(d_shift);
+    if (st) cudaStreamDestroy(st);
+  };
+  auto cuda_ok = [&](cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    rc = set_error(em, ec, e == cudaErrorMemoryAllocation ? AOSB_ERR_MEMORY : AOSB_ERR_CUDA,
+                   "%s failed: %s", what, cudaGetErrorString(e));
+    return false;
+  };
+  const size_t fbytes = aosb_factor_bytes(plan, B);
+  const size_t nL = (size_t)n * L;
+  if (!cuda_ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream") ||
+      !cuda_ok(cudaMalloc(&d_vals, sizeof(float2) * (size_t)B * nnz), "values") ||
+      !cuda_ok(cudaMalloc(&d_rhs_cm, sizeof(float2) * B * nL), "rhs") ||
+      !cuda_ok(cudaMalloc(&d_b, sizeof(double2) * B * nL), "b") ||
+      !cuda_ok(cudaMalloc(&d_x, sizeof(double2) * B * nL), "x") ||
+      !cuda_ok(cudaMalloc(&d_r, sizeof(double2) * B * nL), "r") ||
+      !cuda_ok(cudaMalloc(&d_work, sizeof(float2) * (size_t)B * plan->n_pad * L), "work") ||
+      !cuda_ok(cudaMalloc(&d_factor, fbytes), "factor") ||
+      !cuda_ok(cudaMalloc(&d_piv, sizeof(int32_t) * (size_t)B * plan->n_pad), "pivots") ||
+      !cuda_ok(cudaMalloc(&d_status, sizeof(int32_t) * B), "status") ||
+      !cuda_ok(cudaMalloc(&d_pk, sizeof(int32_t) * B), "pencil index") ||
+      !cuda_ok(cudaMalloc(&d_shift, sizeof(double2) * B), "shifts") ||
+      !cuda_ok(cudaMemcpyAsync(d_vals, req->values, sizeof(float2) * (size_t)B * nnz,
+                               cudaMemcpyHostToDevice, st), "values upload") ||
+      !cuda_ok(cudaMemcpyAsync(d_rhs_cm, req->rhs, sizeof(float2) * B * nL,
+                               cudaMemcpyHostToDevice, st), "rhs upload") ||
+      !cuda_ok(cudaMemsetAsync(d_status, 0, sizeof(int32_t) * B, st), "status") ||
+      !cuda_ok(cudaMemsetAsync(d_shift, 0, sizeof(double2) * B, st), "shifts")) {
+    cleanup();
+    return fail(rc);
+  }
+  iota_kernel<<<ceil_div(B, 64), 64, 0, st>>>(B, d_pk);
+  count_launches(2);
+  {
+    dim3 g(ceil_div((int64_t)nL, 256), B);
+    cm_to_rm_kernel<<<g, 256, 0, st>>>(n, L, d_rhs_cm, d_b);
+  }
+  if (!cuda_ok(cudaStreamSynchronize(st), "upload")) { cleanup(); return fail(rc); }
+  res->upload_seconds = now_seconds() - tu;
+  cudaMemGetInfo(&free_b, &total_b);
+  res->free_device_bytes_after_upload = free_b;
+  res->permanent_device_bytes = fbytes + sizeof(int32_t) * (size_t)B * plan->n_pad;
+  res->peak_device_bytes = res->permanent_device_bytes + sizeof(float2) * (size_t)B * nnz +
+                           sizeof(float2) * B * nL + 3 * sizeof(double2) * B * nL +
+                           sizeof(float2) * (size_t)B * plan->n_pad * L;
+
+  const double tf = now_seconds();
+  aosb_factor_args_v1 fa{AOSPECTRUM_B200_ABI_VERSION, sizeof(aosb_factor_args_v1), B,
+                         AOSB_PRECISION_PLAIN, (const aosb_complex64*)d_vals, nullptr, d_pk,
+                         (const aosb_complex128*)d_shift, d_factor, d_piv, d_status, nullptr, st};
+  if ((rc = aosb_factor(plan, &fa, em, ec)) != 0) { cleanup(); return fail(rc); }
+  if (!cuda_ok(cudaStreamSynchronize(st), "factorization")) { cleanup(); return fail(rc); }
+  res->factorization_seconds = now_seconds() - tf;
+  {
+    std::vector<int32_t> stat(B);
+    cudaMemcpy(stat.data(), d_status, sizeof(int32_t) * B, cudaMemcpyDeviceToHost);
+    for (int b = 0; b < B; ++b)
+      if (stat[b] != 0) {
+        res->engine_status = stat[b];
+        set_error(em, ec, AOSB_ERR_DEVICE_INFO, "factorization of batch entry %d reported status %d",
+                  b, stat[b]);
+        cleanup();
+        return fail(AOSB_ERR_DEVICE_INFO);
+      }
+  }
+  cudaMemGetInfo(&free_b, &total_b);
+  res->free_device_bytes_after_factorization = free_b;
+
+  // Solve + two FP64 refinement steps: x = 0, r = b; repeat {r -> work ->
+  // solve -> x += work; r = b - A x}.
+  const double ts = now_seconds();
+  aosb_solve_args_v1 sa{AOSPECTRUM_B200_ABI_VERSION, sizeof(aosb_solve_args_v1), B, L, 0, 0,
+                        d_factor, d_piv, (aosb_complex64*)d_work, st};
+  const int steps = res->iterative_refinement_steps;
+  for (int it = 0; it <= steps && rc == 0; ++it) {
+    const double2* src = it == 0 ? d_b : d_r;
+    rc = aosb_gather_rhs(plan, B, L, (const aosb_complex128*)src, (int64_t)nL,
+                         (aosb_complex64*)d_work, st, em, ec);
+    if (rc == 0) rc = aosb_solve(plan, &sa, em, ec);
+    if (rc == 0)
+      rc = aosb_scatter_solution(plan, B, L, (const aosb_complex64*)d_work,
+                                 (aosb_complex128*)d_x, it > 0, st, em, ec);
+    if (rc == 0 && it < steps)
+      rc = aosb_shifted_residual(n, L, B, plan->d_indptr, plan->d_indices,
+                                 (const aosb_complex64*)d_vals, nullptr, nnz, d_pk,
+                                 (const aosb_complex128*)d_shift, (const aosb_complex128*)d_b,
+                                 (int64_t)nL, (const aosb_complex128*)d_x,
+                                 (aosb_complex128*)d_r, st, em, ec);
+  }
+  if (rc != 0) { cleanup(); return fail(rc); }
+  {
+    dim3 g(ceil_div((int64_t)nL, 256), B);
+    rm_to_cm_kernel<<<g, 256, 0, st>>>(n, L, d_x, d_rhs_cm);
+    count_launches(1);
+  }
+  if (!cuda_ok(cudaStreamSynchronize(st), "solve")) { cleanup(); return fail(rc); }
+  res->solve_seconds = now_seconds() - ts;
+  cudaMemGetInfo(&free_b, &total_b);
+  res->free_device_bytes_after_solve = free_b;
+  const double td = now_seconds();
+  if (!cuda_ok(cudaMemcpy(req->solution, d_rhs_cm, sizeof(float2) * B * nL,
+                          cudaMemcpyDeviceToHost), "download")) {
+    cleanup();
+    return fail(rc);
+  }
+  res->download_seconds = now_seconds() - td;
+  cleanup();
+  res->total_seconds = now_seconds() - t0;
+  res->status = 0;
+  return 0;
+}
+
+// The tensor-core module provides these when built; see factor_tc.cu.
+}  // extern "C"
+
+extern "C" size_t aosb_factor_workspace_bytes(const aosb_plan_t* plan, int32_t n_pencils,
+                                              int32_t precision) {
+  if (plan == nullptr || n_pencils <= 0) return 0;
+  if (precision == AOSB_PRECISION_BF16X3) return aosb::factor_tc_workspace(plan, n_pencils);
+  return 0;
+}

@@ -1,0 +1,426 @@
+// Numeric tile LU of shifted pencils A_p = H(k_p) - z_p S(k_p) (plain FP32).
+//
+// Storage: factor[p][slot][2][T][T] floats, real plane then imaginary
+// plane, each row-major.  Right-looking over tile steps k:
+//   1. diag_lu: LU of tile (k,k) with partial pivoting inside the tile,
+//      then in-place inversion of both triangles; the slot keeps inv(L_kk)
+//      strictly below the diagonal and inv(U_kk) on and above it.
+//   2. panel:   L_ik = A_ik inv(U_kk)        (i > k, CTA owns row strips)
+//               U_kj = inv(L_kk) P_k A_kj    (j > k, CTA owns column strips)
+//   3. schur:   A_ij -= L_ik U_kj            for every (i, j) target.
+// All kernels batch over pencils (grid.y / grid.x).
+#include "plan.h"
+#include "cgemm.cuh"
+#include "factor.h"
+
+namespace aosb {
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ size_t tile_base(int64_t p, int64_t n_slots, int64_t slot, int T) {
+  return ((size_t)p * (size_t)n_slots + (size_t)slot) * (size_t)(2 * T * T);
+}
+
+// ---------------------------------------------------------------------------
+// Assembly of H - z S into the tile storage (factor must be zeroed first).
+__global__ void assemble_kernel(int64_t n, int64_t nnz, const int64_t* __restrict__ indptr,
+                                const int32_t* __restrict__ indices,
+                                const float2* __restrict__ hv, const float2* __restrict__ sv,
+                                const int32_t* __restrict__ pencil_k,
+                                const double2* __restrict__ shifts,
+                                const int32_t* __restrict__ pinv, const int32_t* __restrict__ slot,
+                                int64_t nb, int64_t n_slots, int T, float* __restrict__ factor) {
+  const int64_t warp = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const int p = blockIdx.y;
+  if (warp >= n) return;
+  const int64_t r = warp;
+  const int64_t kp = pencil_k[p];
+  const double2 zd = shifts[p];
+  const float2 z = make_float2((float)zd.x, (float)zd.y);
+  const float2* h = hv + kp * nnz;
+  const float2* s = sv != nullptr ? sv + kp * nnz : nullptr;
+  const int pr = pinv[r];
+  const int I = pr / T, rr = pr - I * T;
+  for (int64_t e = indptr[r] + lane; e < indptr[r + 1]; e += 32) {
+    const int pc = pinv[indices[e]];
+    const int J = pc / T, cc = pc - J * T;
+    const int sl = slot[(int64_t)I * nb + J];
+    const float2 hval = h[e];
+    const float2 sval = s != nullptr ? s[e] : make_float2(0.f, 0.f);
+    const float re = hval.x - (z.x * sval.x - z.y * sval.y);
+    const float im = hval.y - (z.x * sval.y + z.y * sval.x);
+    const size_t b = tile_base(p, n_slots, sl, T) + (size_t)rr * T + cc;
+    factor[b] = re;
+    factor[b + (size_t)T * T] = im;
+  }
+}
+
+// Padding rows and columns carry an identity diagonal.
+__global__ void pad_identity_kernel(int64_t n_pad, const int32_t* __restrict__ perm,
+                                    const int32_t* __restrict__ diag_slot, int64_t n_slots, int T,
+                                    float* __restrict__ factor) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = blockIdx.y;
+  if (i >= n_pad || perm[i] >= 0) return;
+  const int k = (int)(i / T), r = (int)(i - (int64_t)k * T);
+  factor[tile_base(p, n_slots, diag_slot[k], T) + (size_t)r * T + r] = 1.0f;
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal tile: LU with partial pivoting in shared memory + triangle inverses.
+template <int T>
+__global__ void __launch_bounds__(kThreads) diag_lu_kernel(int k, const int32_t* __restrict__ diag_slot,
+                                                           int64_t n_slots, int64_t n_pad,
+                                                           float* __restrict__ factor,
+                                                           int32_t* __restrict__ pivots,
+                                                           int32_t* __restrict__ status) {
+  extern __shared__ float smem[];
+  float* ar = smem;              // T*T
+  float* ai = smem + T * T;      // T*T
+  float* colr = ai + T * T;      // T  (scratch column)
+  float* coli = colr + T;        // T
+  int* perm = (int*)(coli + T);  // T
+  __shared__ int s_piv;
+  __shared__ float s_pr, s_pi;
+  const int p = blockIdx.x;
+  const int tid = threadIdx.x;
+  float* g = factor + tile_base(p, n_slots, diag_slot[k], T);
+  for (int e = tid; e < T * T; e += kThreads) {
+    ar[e] = g[e];
+    ai[e] = g[e + T * T];
+  }
+  for (int r = tid; r < T; r += kThreads) perm[r] = r;
+  __syncthreads();
+  int bad = 0;
+  for (int j = 0; j < T; ++j) {
+    // Pivot search by warp 0.
+    if (tid < 32) {
+      float best = -1.0f;
+      int bi = j;
+      for (int r = j + tid; r < T; r += 32) {
+        const float m = fabsf(ar[r * T + j]) + fabsf(ai[r * T + j]);
+        if (m > best) { best = m; bi = r; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (tid == 0) s_piv = bi;
+    }
+    __syncthreads();
+    const int pv = s_piv;
+    if (pv != j) {
+      for (int c = tid; c < T; c += kThreads) {
+        float t = ar[j * T + c]; ar[j * T + c] = ar[pv * T + c]; ar[pv * T + c] = t;
+        t = ai[j * T + c]; ai[j * T + c] = ai[pv * T + c]; ai[pv * T + c] = t;
+      }
+      if (tid == 0) { int t = perm[j]; perm[j] = perm[pv]; perm[pv] = t; }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      float pr = ar[j * T + j], pi = ai[j * T + j];
+      float d = pr * pr + pi * pi;
+      if (!(d > 0.0f) || !isfinite(d)) {
+        bad = isfinite(d) ? kDevZeroPivot : kDevNonFinite;
+        pr = 1.0f; pi = 0.0f; d = 1.0f;
+        ar[j * T + j] = 1.0f; ai[j * T + j] = 0.0f;
+      }
+      s_pr = pr / d;
+      s_pi = -pi / d;
+    }
+    __syncthreads();
+    const float ipr = s_pr, ipi = s_pi;
+    for (int r = j + 1 + tid; r < T; r += kThreads) {
+      const float xr = ar[r * T + j], xi = ai[r * T + j];
+      ar[r * T + j] = xr * ipr - xi * ipi;
+      ai[r * T + j] = xr * ipi + xi * ipr;
+    }
+    __syncthreads();
+    const int m = T - j - 1;
+    for (int e = tid; e < m * m; e += kThreads) {
+      const int r = j + 1 + e / m, c = j + 1 + e % m;
+      const float lr = ar[r * T + j], li = ai[r * T + j];
+      const float ur = ar[j * T + c], ui = ai[j * T + c];
+      ar[r * T + c] -= lr * ur - li * ui;
+      ai[r * T + c] -= lr * ui + li * ur;
+    }
+    __syncthreads();
+  }
+  // inv(U): columns left to right; column j of the inverse needs the
+  // already inverted leading block and the original column j.
+  for (int j = 0; j < T; ++j) {
+    for (int r = tid; r <= j; r += kThreads) { colr[r] = ar[r * T + j]; coli[r] = ai[r * T + j]; }
+    __syncthreads();
+    // d = 1 / u_jj
+    const float ur = colr[j], ui = coli[j];
+    const float dd = ur * ur + ui * ui;
+    const float dr = ur / dd, di = -ui / dd;
+    for (int i = tid; i < j; i += kThreads) {
+      float sr = 0.0f, si = 0.0f;
+      for (int q = i; q < j; ++q) {
+        const float xr = ar[i * T + q], xi = ai[i * T + q];
+        sr += xr * colr[q] - xi * coli[q];
+        si += xr * coli[q] + xi * colr[q];
+      }
+      ar[i * T + j] = -(sr * dr - si * di);
+      ai[i * T + j] = -(sr * di + si * dr);
+    }
+    if (tid == 0) { ar[j * T + j] = dr; ai[j * T + j] = di; }
+    __syncthreads();
+  }
+  // inv(L) (unit lower): columns right to left.
+  for (int j = T - 2; j >= 0; --j) {
+    for (int r = j + 1 + tid; r < T; r += kThreads) { colr[r] = ar[r * T + j]; coli[r] = ai[r * T + j]; }
+    __syncthreads();
+    for (int i = j + 1 + tid; i < T; i += kThreads) {
+      // x_i = l_ij + sum_{q=j+1}^{i-1} Linv[i][q] l_qj
+      float sr = colr[i], si = coli[i];
+      for (int q = j + 1; q < i; ++q) {
+        const float xr = ar[i * T + q], xi = ai[i * T + q];
+        sr += xr * colr[q] - xi * coli[q];
+        si += xr * coli[q] + xi * colr[q];
+      }
+      ar[i * T + j] = -sr;
+      ai[i * T + j] = -si;
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < T * T; e += kThreads) {
+    g[e] = ar[e];
+    g[e + T * T] = ai[e];
+  }
+  for (int r = tid; r < T; r += kThreads) pivots[(size_t)p * n_pad + (size_t)k * T + r] = perm[r];
+  if (tid == 0 && bad != 0 && status[p] == 0) status[p] = bad;
+}
+
+// ---------------------------------------------------------------------------
+// Panel updates.  blockIdx.x enumerates (tile, strip); blockIdx.y = pencil.
+// L strips are 32 rows x T columns, U strips are T rows x 32 columns.
+template <int T>
+struct PanelCfg {
+  static constexpr int kStrip = 32;
+  static constexpr int kStrips = T / kStrip;
+  // micro tiles so that (rows / TM) * (cols / TN) == 256
+  static constexpr int LTM = T == 128 ? 4 : 2, LTN = T == 32 ? 2 : 4;   // 32 x T
+  static constexpr int UTM = T == 32 ? 2 : (T == 64 ? 2 : 4), UTN = T == 32 ? 2 : 4;  // T x 32
+  static_assert((32 / LTM) * (T / LTN) == 256, "L panel layout");
+  static_assert((T / UTM) * (32 / UTN) == 256, "U panel layout");
+};
+
+template <int T>
+__global__ void __launch_bounds__(kThreads) panel_kernel(int k, int nL, int nU,
+                                                         const int32_t* __restrict__ lslot,
+                                                         const int32_t* __restrict__ uslot,
+                                                         const int32_t* __restrict__ diag_slot,
+                                                         int64_t n_slots, int64_t n_pad,
+                                                         float* __restrict__ factor,
+                                                         const int32_t* __restrict__ pivots) {
+  using C = PanelCfg<T>;
+  constexpr int S = C::kStrip;
+  constexpr size_t kRaw = sizeof(CgemmSmem<S, T>) > sizeof(CgemmSmem<T, S>)
+                              ? sizeof(CgemmSmem<S, T>) : sizeof(CgemmSmem<T, S>);
+  __shared__ __align__(16) unsigned char raw[kRaw];
+  const int p = blockIdx.y;
+  const int item = blockIdx.x / C::kStrips, strip = blockIdx.x % C::kStrips;
+  const float* D = factor + tile_base(p, n_slots, diag_slot[k], T);
+  if (item < nL) {
+    // rows [strip*S, +S) of A_ik times inv(U_kk) (upper incl. diagonal)
+    constexpr int TM = C::LTM, TN = C::LTN;
+    auto& sm = *reinterpret_cast<CgemmSmem<S, T>*>(raw);
+    float* A = factor + tile_base(p, n_slots, lslot[item], T);
+    float accr[TM][TN] = {}, acci[TM][TN] = {};
+    const int r0 = strip * S;
+    auto la = [&](int m, int q) {
+      const size_t o = (size_t)(r0 + m) * T + q;
+      return make_float2(A[o], A[o + T * T]);
+    };
+    auto lb = [&](int q, int c) {
+      if (q > c) return make_float2(0.f, 0.f);
+      const size_t o = (size_t)q * T + c;
+      return make_float2(D[o], D[o + T * T]);
+    };
+    cgemm_cta<S, T, TM, TN>(accr, acci, T, sm, la, lb);
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) {
+        const size_t o = (size_t)(r0 + cg_row<S, T, TM, TN>(i)) * T + cg_col<S, T, TM, TN>(j);
+        A[o] = accr[i][j];
+        A[o + T * T] = acci[i][j];
+      }
+  } else if (item < nL + nU) {
+    // columns [strip*S, +S) of inv(L_kk) (P_k A_kj)
+    constexpr int TM = C::UTM, TN = C::UTN;
+    auto& sm = *reinterpret_cast<CgemmSmem<T, S>*>(raw);
+    float* A = factor + tile_base(p, n_slots, uslot[item - nL], T);
+    const int32_t* pv = pivots + (size_t)p * n_pad + (size_t)k * T;
+    float accr[TM][TN] = {}, acci[TM][TN] = {};
+    const int c0 = strip * S;
+    auto la = [&](int r, int q) {
+      if (q > r) return make_float2(0.f, 0.f);
+      if (q == r) return make_float2(1.f, 0.f);
+      const size_t o = (size_t)r * T + q;
+      return make_float2(D[o], D[o + T * T]);
+    };
+    auto lb = [&](int q, int c) {
+      const size_t o = (size_t)pv[q] * T + c0 + c;
+      return make_float2(A[o], A[o + T * T]);
+    };
+    cgemm_cta<T, S, TM, TN>(accr, acci, T, sm, la, lb);
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) {
+        const size_t o = (size_t)cg_row<T, S, TM, TN>(i) * T + c0 + cg_col<T, S, TM, TN>(j);
+        A[o] = accr[i][j];
+        A[o + T * T] = acci[i][j];
+      }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Schur update: blockIdx.x = (pair, sub-block), blockIdx.y = pencil.
+template <int T>
+struct SchurCfg {
+  static constexpr int BM = T >= 64 ? 64 : 32;
+  static constexpr int BN = T >= 64 ? 64 : 32;
+  static constexpr int TM = T >= 64 ? 4 : 2;
+  static constexpr int TN = T >= 64 ? 4 : 2;
+  static constexpr int kSub = (T / BM) * (T / BN);
+};
+
+template <int T>
+__global__ void __launch_bounds__(kThreads) schur_kernel(int nU, const int32_t* __restrict__ lslot,
+                                                         const int32_t* __restrict__ uslot,
+                                                         const int32_t* __restrict__ tslot,
+                                                         int64_t n_slots, float* __restrict__ factor) {
+  using C = SchurCfg<T>;
+  constexpr int BM = C::BM, BN = C::BN, TM = C::TM, TN = C::TN;
+  __shared__ CgemmSmem<BM, BN> sm;
+  const int p = blockIdx.y;
+  const int pair = blockIdx.x / C::kSub, sub = blockIdx.x % C::kSub;
+  const int a = pair / nU, b = pair % nU;
+  const int m0 = (sub / (T / BN)) * BM, n0 = (sub % (T / BN)) * BN;
+  const float* L = factor + tile_base(p, n_slots, lslot[a], T);
+  const float* U = factor + tile_base(p, n_slots, uslot[b], T);
+  float* Cc = factor + tile_base(p, n_slots, tslot[pair], T);
+  float accr[TM][TN] = {}, acci[TM][TN] = {};
+  auto la = [&](int m, int q) {
+    const size_t o = (size_t)(m0 + m) * T + q;
+    return make_float2(L[o], L[o + T * T]);
+  };
+  auto lb = [&](int q, int c) {
+    const size_t o = (size_t)q * T + n0 + c;
+    return make_float2(U[o], U[o + T * T]);
+  };
+  cgemm_cta<BM, BN, TM, TN>(accr, acci, T, sm, la, lb);
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const size_t o = (size_t)(m0 + cg_row<BM, BN, TM, TN>(i)) * T + n0 + cg_col<BM, BN, TM, TN>(j);
+      Cc[o] -= accr[i][j];
+      Cc[o + T * T] -= acci[i][j];
+    }
+}
+
+template <int T>
+int run_plain(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
+  cudaStream_t st = (cudaStream_t)a->stream;
+  const int np = a->n_pencils;
+  const size_t diag_smem = (size_t)(2 * T * T + 2 * T) * sizeof(float) + T * sizeof(int);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(diag_lu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)diag_smem);
+    if (e != cudaSuccess)
+      return set_error(err, cap, AOSB_ERR_CUDA, "diag_lu smem attribute: %s", cudaGetErrorString(e));
+    attr_done = true;
+  }
+  for (int64_t k = 0; k < P->nb; ++k) {
+    diag_lu_kernel<T><<<np, kThreads, diag_smem, st>>>((int)k, P->d_diag_slot, P->n_slots, P->n_pad,
+                                                      a->factor, a->pivots, a->status);
+    count_launches(1);
+    const int nL = P->lb_off[k + 1] - P->lb_off[k];
+    const int nU = P->ur_off[k + 1] - P->ur_off[k];
+    if (nL + nU > 0) {
+      dim3 grid((unsigned)((nL + nU) * PanelCfg<T>::kStrips), np);
+      panel_kernel<T><<<grid, kThreads, 0, st>>>((int)k, nL, nU, P->d_lb_slot + P->lb_off[k],
+                                                 P->d_ur_slot + P->ur_off[k], P->d_diag_slot,
+                                                 P->n_slots, P->n_pad, a->factor, a->pivots);
+      count_launches(1);
+    }
+    if (nL > 0 && nU > 0) {
+      const int64_t blocks = (int64_t)nL * nU * SchurCfg<T>::kSub;
+      if (blocks > INT32_MAX) return set_error(err, cap, AOSB_ERR_SIZE, "schur grid too large");
+      dim3 grid((unsigned)blocks, np);
+      schur_kernel<T><<<grid, kThreads, 0, st>>>(nU, P->d_lb_slot + P->lb_off[k],
+                                                 P->d_ur_slot + P->ur_off[k],
+                                                 P->d_sc_slot + P->sc_off[k], P->n_slots, a->factor);
+      count_launches(1);
+    }
+  }
+  return launch_check(err, cap, "plain factorization");
+}
+
+}  // namespace
+
+int factor_assemble(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
+  cudaStream_t st = (cudaStream_t)a->stream;
+  const int np = a->n_pencils;
+  const size_t bytes = (size_t)np * P->n_slots * 2 * P->T * P->T * sizeof(float);
+  AOSB_CUDA_TRY(cudaMemsetAsync(a->factor, 0, bytes, st), err, cap);
+  dim3 g1(ceil_div(P->n, 8), np);
+  assemble_kernel<<<g1, 256, 0, st>>>(P->n, P->nnz, P->d_indptr, P->d_indices,
+                                      (const float2*)a->h_values, (const float2*)a->s_values,
+                                      a->pencil_k, (const double2*)a->shifts, P->d_pinv, P->d_slot,
+                                      P->nb, P->n_slots, (int)P->T, a->factor);
+  dim3 g2(ceil_div(P->n_pad, 256), np);
+  pad_identity_kernel<<<g2, 256, 0, st>>>(P->n_pad, P->d_perm, P->d_diag_slot, P->n_slots,
+                                          (int)P->T, a->factor);
+  count_launches(2);
+  return launch_check(err, cap, "assemble");
+}
+
+int factor_plain(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
+  switch (P->T) {
+    case 32: return run_plain<32>(P, a, err, cap);
+    case 64: return run_plain<64>(P, a, err, cap);
+    case 128: return run_plain<128>(P, a, err, cap);
+  }
+  return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "unsupported tile size");
+}
+
+}  // namespace aosb
+
+extern "C" {
+
+size_t aosb_factor_bytes(const aosb_plan_t* p, int32_t n_pencils) {
+  if (p == nullptr || n_pencils <= 0) return 0;
+  return (size_t)n_pencils * (size_t)p->n_slots * (size_t)(2 * p->T * p->T) * sizeof(float);
+}
+
+int aosb_factor(const aosb_plan_t* plan, const aosb_factor_args_v1* a, char* err, size_t cap) {
+  using aosb::set_error;
+  if (plan == nullptr || a == nullptr) return set_error(err, cap, AOSB_ERR_NULL, "null argument");
+  if (a->abi_version != AOSPECTRUM_B200_ABI_VERSION || a->struct_size != sizeof(*a))
+    return set_error(err, cap, AOSB_ERR_ABI, "factor args ABI mismatch");
+  if (a->n_pencils <= 0 || a->n_pencils > 65535)
+    return set_error(err, cap, AOSB_ERR_BATCH, "n_pencils must be in 1..65535");
+  if (a->h_values == nullptr || a->pencil_k == nullptr ||
+      a->shifts == nullptr || a->factor == nullptr || a->pivots == nullptr || a->status == nullptr)
+    return set_error(err, cap, AOSB_ERR_NULL, "required pointer is null");
+  if (!plan->uploaded)
+    return set_error(err, cap, AOSB_ERR_ARGUMENT, "call aosb_plan_upload first");
+  int rc = aosb::factor_assemble(plan, a, err, cap);
+  if (rc) return rc;
+  if (a->precision == AOSB_PRECISION_PLAIN) return aosb::factor_plain(plan, a, err, cap);
+  if (a->precision == AOSB_PRECISION_BF16X3) return aosb::factor_tc(plan, a, err, cap);
+  return set_error(err, cap, AOSB_ERR_ARGUMENT, "unknown precision %d", a->precision);
+}
+
+}  // extern "C"

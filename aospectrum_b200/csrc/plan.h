@@ -1,0 +1,40 @@
+// Symbolic plan shared by the factorization and solve modules.
+#pragma once
+
+#include "common.cuh"
+
+#include <vector>
+
+struct aosb_plan {
+  int64_t n = 0, n_pad = 0, nnz = 0, nb = 0, T = 0, n_slots = 0;
+  int64_t n_sv = 0, n_nodes = 0, schur_updates = 0, tree_levels = 0;
+  double flops = 0.0, flops_alg = 0.0;
+  std::vector<int32_t> perm;  // n_pad
+  std::vector<int32_t> pinv;  // n
+  std::vector<int32_t> slot;  // nb*nb
+  std::vector<int32_t> real_dofs;  // per tile
+  // Per-step tile lists: offsets [nb+1] and (tile, slot) entries.
+  std::vector<int32_t> lb_off, lb_tile, lb_slot;  // L column k, rows i > k
+  std::vector<int32_t> ur_off, ur_tile, ur_slot;  // U row k, cols j > k
+  std::vector<int32_t> ua_off, ua_tile, ua_slot;  // U column k, rows i < k
+  std::vector<int32_t> ll_off, ll_tile, ll_slot;  // L row k, cols j < k
+  std::vector<int64_t> sc_off;                    // Schur target offsets [nb+1]
+  std::vector<int32_t> sc_slot;                   // |L_k| x |U_k| target slots per step
+  std::vector<int32_t> diag_slot;                 // slot of (k, k)
+  // Device copies.
+  int32_t *d_perm = nullptr, *d_pinv = nullptr, *d_slot = nullptr;
+  int32_t *d_lb_slot = nullptr, *d_ur_slot = nullptr, *d_ua_slot = nullptr, *d_ll_slot = nullptr;
+  int32_t *d_lb_tile = nullptr, *d_ur_tile = nullptr, *d_ua_tile = nullptr, *d_ll_tile = nullptr;
+  int32_t *d_sc_slot = nullptr, *d_diag_slot = nullptr;
+  // Pattern copies for the shifted-value assembly (host and device).
+  std::vector<int64_t> h_indptr;
+  std::vector<int32_t> h_indices;
+  bool uploaded = false;
+  int64_t* d_indptr = nullptr;
+  int32_t* d_indices = nullptr;
+};
+
+namespace aosb {
+int plan_upload(aosb_plan* p, char* err, size_t cap);
+void plan_free_device(aosb_plan* p);
+}  // namespace aosb

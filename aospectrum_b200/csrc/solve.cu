@@ -1,0 +1,345 @@
+// Block-RHS triangular solves with the tile factors, plus the gather /
+// scatter between the original dof order (complex128) and the permuted,
+// padded solver order (complex64), and the FP64 shifted residual used by
+// iterative refinement.
+//
+// With P A = L U (P block diagonal, one permutation per tile row):
+//   A X = B    forward  y_k = inv(L_kk) P_k (b_k - sum_{j<k} L_kj y_j)
+//              backward x_k = inv(U_kk) (y_k - sum_{j>k} U_kj x_j)
+//   A^H X = B  forward  w_k = inv(U_kk)^H (b_k - sum_{j<k} U_jk^H w_j)
+//              backward x_k = P_k^T inv(L_kk)^H (w_k - sum_{j>k} L_jk^H x_j)
+// (the stored L_kj, j < k, are in the row order of tile row k before its
+// own pivoting, which is why P_k is applied after the accumulation.)
+// Each sweep is right-looking: a diagonal kernel per step, then an update
+// kernel for every off-diagonal tile of that step.
+#include "plan.h"
+#include "cgemm.cuh"
+
+namespace aosb {
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ size_t tile_base(int64_t p, int64_t n_slots, int64_t slot, int T) {
+  return ((size_t)p * (size_t)n_slots + (size_t)slot) * (size_t)(2 * T * T);
+}
+
+enum DiagOp { kLinv = 0, kUinv = 1, kUinvH = 2, kLinvH = 3 };
+
+// Diagonal step: X_k <- op(D_kk) X_k over column strip blockIdx.x of width 32.
+// kLinv gathers rows through P_k first; kLinvH scatters rows through P_k^T.
+template <int T, int OP>
+__global__ void __launch_bounds__(kThreads) solve_diag_kernel(int k, int nrhs, int64_t n_pad,
+                                                              const int32_t* __restrict__ diag_slot,
+                                                              int64_t n_slots,
+                                                              const float* __restrict__ factor,
+                                                              const int32_t* __restrict__ pivots,
+                                                              float2* __restrict__ work) {
+  constexpr int BN = 32;
+  constexpr int TN = T == 32 ? 2 : 4;
+  constexpr int TM = (T / 4) * (BN / TN) == 256 ? 4 : ((T / 2) * (BN / TN) == 256 ? 2 : 1);
+  static_assert((T / TM) * (BN / TN) == 256, "layout");
+  __shared__ CgemmSmem<T, BN> sm;
+  const int p = blockIdx.y;
+  const int c0 = blockIdx.x * BN;
+  const float* D = factor + tile_base(p, n_slots, diag_slot[k], T);
+  const int32_t* pv = pivots + (size_t)p * n_pad + (size_t)k * T;
+  float2* X = work + ((size_t)p * n_pad + (size_t)k * T) * nrhs;
+  float accr[TM][TN] = {}, acci[TM][TN] = {};
+  auto la = [&](int r, int q) -> float2 {
+    if (OP == kLinv) {
+      if (q > r) return make_float2(0.f, 0.f);
+      if (q == r) return make_float2(1.f, 0.f);
+      const size_t o = (size_t)r * T + q;
+      return make_float2(D[o], D[o + T * T]);
+    } else if (OP == kUinv) {
+      if (q < r) return make_float2(0.f, 0.f);
+      const size_t o = (size_t)r * T + q;
+      return make_float2(D[o], D[o + T * T]);
+    } else if (OP == kUinvH) {  // conj(Uinv[q][r]), nonzero for q <= r
+      if (q > r) return make_float2(0.f, 0.f);
+      const size_t o = (size_t)q * T + r;
+      return make_float2(D[o], -D[o + T * T]);
+    } else {  // kLinvH: conj(Linv[q][r]), unit diagonal, nonzero for q >= r
+      if (q < r) return make_float2(0.f, 0.f);
+      if (q == r) return make_float2(1.f, 0.f);
+      const size_t o = (size_t)q * T + r;
+      return make_float2(D[o], -D[o + T * T]);
+    }
+  };
+  auto lb = [&](int q, int c) -> float2 {
+    const int col = c0 + c;
+    if (col >= nrhs) return make_float2(0.f, 0.f);
+    const int row = OP == kLinv ? pv[q] : q;
+    return X[(size_t)row * nrhs + col];
+  };
+  cgemm_cta<T, BN, TM, TN>(accr, acci, T, sm, la, lb);
+  // Every CTA has read its whole column strip before this point.
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const int r = cg_row<T, BN, TM, TN>(i), col = c0 + cg_col<T, BN, TM, TN>(j);
+      if (col >= nrhs) continue;
+      const int row = OP == kLinvH ? pv[r] : r;
+      X[(size_t)row * nrhs + col] = make_float2(accr[i][j], acci[i][j]);
+    }
+}
+
+enum UpdOp { kPlain = 0, kConjT = 1 };
+
+// Update step: X_i -= op(F_t) X_k for the listed tiles.  blockIdx.x =
+// (item, row half, column strip); op = plain tile or conjugate transpose.
+template <int T, int OP>
+__global__ void __launch_bounds__(kThreads) solve_update_kernel(
+    int k, int n_items, int nrhs, int64_t n_pad, const int32_t* __restrict__ tiles,
+    const int32_t* __restrict__ slots, int64_t n_slots, const float* __restrict__ factor,
+    float2* __restrict__ work) {
+  constexpr int BM = T >= 64 ? 64 : 32;
+  constexpr int BN = 32;
+  constexpr int TM = BM == 64 ? 4 : 2, TN = BM == 64 ? 2 : 2;
+  static_assert((BM / TM) * (BN / TN) == 256, "layout");
+  constexpr int kRowBlocks = T / BM;
+  __shared__ CgemmSmem<BM, BN> sm;
+  const int p = blockIdx.y;
+  const int ncs = (nrhs + BN - 1) / BN;
+  const int item = blockIdx.x / (kRowBlocks * ncs);
+  const int rem = blockIdx.x % (kRowBlocks * ncs);
+  const int m0 = (rem / ncs) * BM, c0 = (rem % ncs) * BN;
+  if (item >= n_items) return;
+  const int i = tiles[item];
+  const float* F = factor + tile_base(p, n_slots, slots[item], T);
+  const float2* Xk = work + ((size_t)p * n_pad + (size_t)k * T) * nrhs;
+  float2* Xi = work + ((size_t)p * n_pad + (size_t)i * T) * nrhs;
+  float accr[TM][TN] = {}, acci[TM][TN] = {};
+  auto la = [&](int m, int q) -> float2 {
+    if (OP == kPlain) {
+      const size_t o = (size_t)(m0 + m) * T + q;
+      return make_float2(F[o], F[o + T * T]);
+    } else {
+      const size_t o = (size_t)q * T + (m0 + m);
+      return make_float2(F[o], -F[o + T * T]);
+    }
+  };
+  auto lb = [&](int q, int c) -> float2 {
+    const int col = c0 + c;
+    if (col >= nrhs) return make_float2(0.f, 0.f);
+    return Xk[(size_t)q * nrhs + col];
+  };
+  cgemm_cta<BM, BN, TM, TN>(accr, acci, T, sm, la, lb);
+#pragma unroll
+  for (int a = 0; a < TM; ++a)
+#pragma unroll
+    for (int b = 0; b < TN; ++b) {
+      const int r = m0 + cg_row<BM, BN, TM, TN>(a), col = c0 + cg_col<BM, BN, TM, TN>(b);
+      if (col >= nrhs) continue;
+      float2 v = Xi[(size_t)r * nrhs + col];
+      v.x -= accr[a][b];
+      v.y -= acci[a][b];
+      Xi[(size_t)r * nrhs + col] = v;
+    }
+}
+
+template <int T>
+int run_solve(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t cap) {
+  cudaStream_t st = (cudaStream_t)a->stream;
+  const int np = a->n_pencils, L = a->n_rhs;
+  const int ncs = (L + 31) / 32;
+  constexpr int BM = T >= 64 ? 64 : 32;
+  const int rowblocks = T / BM;
+  float2* W = (float2*)a->work;
+  auto diag = [&](int k, int op) {
+    count_launches(1);
+    dim3 g(ncs, np);
+    switch (op) {
+      case kLinv: solve_diag_kernel<T, kLinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W); break;
+      case kUinv: solve_diag_kernel<T, kUinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W); break;
+      case kUinvH: solve_diag_kernel<T, kUinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W); break;
+      default: solve_diag_kernel<T, kLinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W); break;
+    }
+  };
+  auto update = [&](int k, const std::vector<int32_t>& off, const int32_t* dtiles,
+                    const int32_t* dslots, int op) {
+    const int n = off[k + 1] - off[k];
+    if (n == 0) return;
+    dim3 g((unsigned)(n * rowblocks * ncs), np);
+    count_launches(1);
+    if (op == kPlain)
+      solve_update_kernel<T, kPlain><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + off[k], dslots + off[k], P->n_slots, a->factor, W);
+    else
+      solve_update_kernel<T, kConjT><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + off[k], dslots + off[k], P->n_slots, a->factor, W);
+  };
+  const int nb = (int)P->nb;
+  if (!a->adjoint) {
+    for (int k = 0; k < nb; ++k) {
+      diag(k, kLinv);
+      update(k, P->lb_off, P->d_lb_tile, P->d_lb_slot, kPlain);
+    }
+    for (int k = nb - 1; k >= 0; --k) {
+      diag(k, kUinv);
+      update(k, P->ua_off, P->d_ua_tile, P->d_ua_slot, kPlain);
+    }
+  } else {
+    for (int k = 0; k < nb; ++k) {
+      diag(k, kUinvH);
+      // X_i -= U_ki^H w_k for U tiles (k, i), i > k
+      update(k, P->ur_off, P->d_ur_tile, P->d_ur_slot, kConjT);
+    }
+    for (int k = nb - 1; k >= 0; --k) {
+      diag(k, kLinvH);
+      // X_i -= L_ki^H x_k for L tiles (k, i), i < k
+      update(k, P->ll_off, P->d_ll_tile, P->d_ll_slot, kConjT);
+    }
+  }
+  return launch_check(err, cap, "solve");
+}
+
+__global__ void gather_rhs_kernel(int64_t n_pad, int nrhs, const int32_t* __restrict__ perm,
+                                  const double2* __restrict__ src, int64_t src_stride,
+                                  float2* __restrict__ work) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = blockIdx.y;
+  if (idx >= n_pad * nrhs) return;
+  const int64_t i = idx / nrhs, c = idx - (idx / nrhs) * nrhs;
+  const int32_t o = perm[i];
+  float2 v = make_float2(0.f, 0.f);
+  if (o >= 0) {
+    const double2 s = src[(size_t)p * src_stride + (size_t)o * nrhs + c];
+    v = make_float2((float)s.x, (float)s.y);
+  }
+  work[((size_t)p * n_pad) * nrhs + idx] = v;
+}
+
+__global__ void scatter_solution_kernel(int64_t n, int64_t n_pad, int nrhs,
+                                        const int32_t* __restrict__ pinv,
+                                        const float2* __restrict__ work, double2* __restrict__ x,
+                                        int accumulate) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = blockIdx.y;
+  if (idx >= n * nrhs) return;
+  const int64_t j = idx / nrhs, c = idx - (idx / nrhs) * nrhs;
+  const float2 w = work[((size_t)p * n_pad + pinv[j]) * nrhs + c];
+  double2* o = x + (size_t)p * n * nrhs + idx;
+  if (accumulate) {
+    double2 v = *o;
+    v.x += (double)w.x;
+    v.y += (double)w.y;
+    *o = v;
+  } else {
+    *o = make_double2((double)w.x, (double)w.y);
+  }
+}
+
+// r = b - (H - z S) x, one warp per row, lanes over right-hand sides.
+__global__ void shifted_residual_kernel(int64_t n, int nrhs, const int64_t* __restrict__ indptr,
+                                        const int32_t* __restrict__ indices,
+                                        const float2* __restrict__ hv,
+                                        const float2* __restrict__ sv, int64_t nnz,
+                                        const int32_t* __restrict__ pencil_k,
+                                        const double2* __restrict__ shifts,
+                                        const double2* __restrict__ b, int64_t b_stride,
+                                        const double2* __restrict__ x, double2* __restrict__ r) {
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const int p = blockIdx.y;
+  if (row >= n) return;
+  const int64_t kp = pencil_k[p];
+  const double2 z = shifts[p];
+  const float2* h = hv + kp * nnz;
+  const float2* s = sv != nullptr ? sv + kp * nnz : nullptr;
+  const double2* xp = x + (size_t)p * n * nrhs;
+  for (int c0 = 0; c0 < nrhs; c0 += 32) {
+    const int c = c0 + lane;
+    double hr = 0, hi = 0, sr = 0, si = 0;
+    if (c < nrhs) {
+      for (int64_t e = indptr[row]; e < indptr[row + 1]; ++e) {
+        const int64_t col = indices[e];
+        const float2 hh = h[e];
+        const float2 ss = s != nullptr ? s[e] : make_float2(0.f, 0.f);
+        const double2 xv = xp[(size_t)col * nrhs + c];
+        hr += (double)hh.x * xv.x - (double)hh.y * xv.y;
+        hi += (double)hh.x * xv.y + (double)hh.y * xv.x;
+        sr += (double)ss.x * xv.x - (double)ss.y * xv.y;
+        si += (double)ss.x * xv.y + (double)ss.y * xv.x;
+      }
+      // A x = H x - z (S x)
+      const double ar = hr - (z.x * sr - z.y * si);
+      const double ai = hi - (z.x * si + z.y * sr);
+      const double2 bv = b[(size_t)p * b_stride + (size_t)row * nrhs + c];
+      r[((size_t)p * n + row) * nrhs + c] = make_double2(bv.x - ar, bv.y - ai);
+    }
+  }
+}
+
+}  // namespace
+}  // namespace aosb
+
+extern "C" {
+
+int aosb_solve(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* err, size_t cap) {
+  using aosb::set_error;
+  if (P == nullptr || a == nullptr) return set_error(err, cap, AOSB_ERR_NULL, "null argument");
+  if (a->abi_version != AOSPECTRUM_B200_ABI_VERSION || a->struct_size != sizeof(*a))
+    return set_error(err, cap, AOSB_ERR_ABI, "solve args ABI mismatch");
+  if (a->n_pencils <= 0 || a->n_pencils > 65535 || a->n_rhs <= 0 || a->n_rhs > 256)
+    return set_error(err, cap, AOSB_ERR_BATCH, "invalid pencil or right-hand-side count");
+  if (a->factor == nullptr || a->pivots == nullptr || a->work == nullptr)
+    return set_error(err, cap, AOSB_ERR_NULL, "required pointer is null");
+  if (!P->uploaded) return set_error(err, cap, AOSB_ERR_ARGUMENT, "call aosb_plan_upload first");
+  switch (P->T) {
+    case 32: return aosb::run_solve<32>(P, a, err, cap);
+    case 64: return aosb::run_solve<64>(P, a, err, cap);
+    case 128: return aosb::run_solve<128>(P, a, err, cap);
+  }
+  return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "unsupported tile size");
+}
+
+int aosb_gather_rhs(const aosb_plan_t* P, int32_t np, int32_t nrhs, const aosb_complex128* src,
+                    int64_t src_stride, aosb_complex64* work, void* stream, char* err, size_t cap) {
+  if (P == nullptr || src == nullptr || work == nullptr)
+    return aosb::set_error(err, cap, AOSB_ERR_NULL, "null argument");
+  if (!P->uploaded) return aosb::set_error(err, cap, AOSB_ERR_ARGUMENT, "plan not uploaded");
+  if (np <= 0 || np > 65535 || nrhs <= 0)
+    return aosb::set_error(err, cap, AOSB_ERR_BATCH, "invalid batch");
+  dim3 g(aosb::ceil_div(P->n_pad * nrhs, 256), np);
+  aosb::gather_rhs_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(
+      P->n_pad, nrhs, P->d_perm, (const double2*)src, src_stride, (float2*)work);
+  aosb::count_launches(1);
+  return aosb::launch_check(err, cap, "gather_rhs");
+}
+
+int aosb_scatter_solution(const aosb_plan_t* P, int32_t np, int32_t nrhs,
+                          const aosb_complex64* work, aosb_complex128* x, int32_t accumulate,
+                          void* stream, char* err, size_t cap) {
+  if (P == nullptr || work == nullptr || x == nullptr)
+    return aosb::set_error(err, cap, AOSB_ERR_NULL, "null argument");
+  if (!P->uploaded) return aosb::set_error(err, cap, AOSB_ERR_ARGUMENT, "plan not uploaded");
+  if (np <= 0 || np > 65535 || nrhs <= 0)
+    return aosb::set_error(err, cap, AOSB_ERR_BATCH, "invalid batch");
+  dim3 g(aosb::ceil_div(P->n * nrhs, 256), np);
+  aosb::scatter_solution_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(
+      P->n, P->n_pad, nrhs, P->d_pinv, (const float2*)work, (double2*)x, accumulate);
+  aosb::count_launches(1);
+  return aosb::launch_check(err, cap, "scatter_solution");
+}
+
+int aosb_shifted_residual(int64_t n, int32_t nrhs, int32_t np, const int64_t* indptr,
+                          const int32_t* indices, const aosb_complex64* h_values,
+                          const aosb_complex64* s_values, int64_t nnz, const int32_t* pencil_k,
+                          const aosb_complex128* shifts, const aosb_complex128* b,
+                          int64_t b_stride, const aosb_complex128* x, aosb_complex128* r,
+                          void* stream, char* err, size_t cap) {
+  if (indptr == nullptr || indices == nullptr || h_values == nullptr ||
+      pencil_k == nullptr || shifts == nullptr || b == nullptr || x == nullptr || r == nullptr)
+    return aosb::set_error(err, cap, AOSB_ERR_NULL, "null argument");
+  if (np <= 0 || np > 65535 || nrhs <= 0 || n <= 0)
+    return aosb::set_error(err, cap, AOSB_ERR_BATCH, "invalid batch");
+  dim3 g(aosb::ceil_div(n, 8), np);
+  aosb::shifted_residual_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(
+      n, nrhs, indptr, indices, (const float2*)h_values, (const float2*)s_values, nnz, pencil_k,
+      (const double2*)shifts, (const double2*)b, b_stride, (const double2*)x, (double2*)r);
+  aosb::count_launches(1);
+  return aosb::launch_check(err, cap, "shifted_residual");
+}
+
+}  // extern "C"

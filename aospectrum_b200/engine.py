@@ -1,0 +1,530 @@
+"""GPU Band engine: device-resident bundle, Bloch sums and batched CISS.
+
+One ``BandEngine`` per (bundle, process, GPU).  Construction uploads the
+operator block values once, builds the CSR pattern (``aosb_bloch_create``)
+and the symbolic plan (``aosb_plan_create``, once per bundle).  Each call of
+``solve_kpoints`` then runs, for a group of k points:
+
+1. Bloch sums H(k), S(k) on the device (bit-identical to the reference
+   numpy path for real block values);
+2. rhs = S(k) Q in FP64 with the reference's probe block Q;
+3. every (k, contour node) pencil through batched tile factorizations; in
+   "mixed" precision a node and its conjugate partner share one
+   factorization (A^H = H - conj(z) S), the Schur updates run on the tensor
+   cores in split BF16, and every solve gets FP64 iterative refinement;
+4. moment accumulation, S-Gram rank truncation, Rayleigh-Ritz, ghost
+   filter and FP64 residuals.
+
+This replaces ``BlochWorkspace.update`` + ``CudssCissSolver.solve_interval``
+of the reference (``src/aospectrum/sparse.py:199-245``,
+``src/aospectrum/ciss.py:266-391``).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from time import perf_counter
+from typing import Any, Sequence
+
+import numpy as np
+
+from . import native
+from .ciss import (
+    CissResult,
+    CissSettings,
+    EngineSettings,
+    contour_geometry,
+    moment_coefficients,
+    nonspurious_mask,
+    probe_block,
+    projected_eigh,
+    result_warnings,
+    truncate_gram,
+)
+from .data import EnergyInterval, LocalizedOperatorBundle
+from .errors import InputError, SolverError
+from .sparse import SparsePair
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise SolverError("the B200 Band engine needs a CUDA device")
+    return torch
+
+
+def choose_tile(n: int) -> int:
+    if n <= 256:
+        return 32
+    if n <= 4096:
+        return 64
+    return 128
+
+
+@dataclass
+class PlanSummary:
+    n: int
+    n_pad: int
+    nnz: int
+    tile: int
+    n_tiles: int
+    n_slots: int
+    n_nodes: int
+    tree_levels: int
+    factor_flops: float
+    factor_flops_alg: float
+    factor_bytes: float
+
+
+class BlochDevice:
+    """CSR pattern of a bundle plus device-resident block values."""
+
+    def __init__(self, bundle: LocalizedOperatorBundle, device: Any) -> None:
+        torch = _torch()
+        lib = native.library()
+        ops = bundle.operators
+        self.n = bundle.n_orbitals
+        offsets = np.ascontiguousarray(bundle.basis.atom_offsets, dtype=np.int64)
+        rows = np.ascontiguousarray(ops.row_atom, dtype=np.int32)
+        cols = np.ascontiguousarray(ops.col_atom, dtype=np.int32)
+        shifts = np.ascontiguousarray(ops.lattice_shift, dtype=np.int32)
+        boff = np.ascontiguousarray(ops.block_offsets, dtype=np.int64)
+        handle = native.c_vp()
+        with torch.cuda.device(device):
+            native.call("aosb_bloch_create", self.n, bundle.basis.n_atoms, offsets.ctypes.data,
+                        ops.n_blocks, rows.ctypes.data, cols.ctypes.data, shifts.ctypes.data,
+                        boff.ctypes.data, native.C.byref(handle))
+        self.handle = handle
+        with torch.cuda.device(device):
+            native.call("aosb_bloch_upload", handle)
+        nnz, nsh = native.c_i64(), native.c_i64()
+        lib.aosb_bloch_info(handle, native.C.byref(nnz), native.C.byref(nsh))
+        self.nnz, self.n_shifts = int(nnz.value), int(nsh.value)
+        self.indptr = np.empty(self.n + 1, dtype=np.int64)
+        self.indices = np.empty(self.nnz, dtype=np.int32)
+        self.shifts = np.empty((self.n_shifts, 3), dtype=np.int32)
+        self.block_shift = np.empty(ops.n_blocks, dtype=np.int32)
+        lib.aosb_bloch_export(handle, self.indptr.ctypes.data, self.indices.ctypes.data,
+                              self.shifts.ctypes.data, self.block_shift.ctypes.data)
+        dptr, dind = native.c_vp(), native.c_vp()
+        lib.aosb_bloch_device_pattern(handle, native.C.byref(dptr), native.C.byref(dind))
+        self.d_indptr, self.d_indices = int(dptr.value), int(dind.value)
+        complex_values = np.iscomplexobj(ops.h_values) or np.iscomplexobj(ops.s_values)
+        self.value_kind = 1 if complex_values else 0
+        dtype = np.complex64 if complex_values else np.float32
+        hv = np.array(ops.h_values, dtype=dtype, copy=True)
+        sv = np.array(ops.s_values, dtype=dtype, copy=True)
+        tdt = torch.complex64 if complex_values else torch.float32
+        self.h_values = torch.from_numpy(hv).to(device=device, dtype=tdt)
+        self.s_values = torch.from_numpy(sv).to(device=device, dtype=tdt)
+        self.device = device
+
+    def phases(self, kpoints: np.ndarray) -> np.ndarray:
+        """exp(2 pi i R.k) per k and distinct shift, with the reference's
+        complex64 arithmetic (sparse.py:207-213)."""
+        out = np.empty((len(kpoints), self.n_shifts), dtype=np.complex64)
+        r = self.shifts.astype(np.float32)
+        for i, k in enumerate(kpoints):
+            arg = r @ np.asarray(k, dtype=np.float32)
+            out[i] = np.exp(np.asarray(2.0j * np.pi, dtype=np.complex64) * arg)
+        return out
+
+    def apply(self, kpoints: np.ndarray, stream: Any = None):
+        """Device H(k), S(k) values [n_k, nnz] complex64."""
+        torch = _torch()
+        nk = len(kpoints)
+        ph = torch.from_numpy(self.phases(kpoints)).to(self.device, non_blocking=False)
+        h = torch.empty((nk, self.nnz), dtype=torch.complex64, device=self.device)
+        s = torch.empty_like(h)
+        st = torch.cuda.current_stream(self.device).cuda_stream if stream is None else stream
+        native.call("aosb_bloch_apply", self.handle, self.value_kind, self.h_values.data_ptr(),
+                    self.s_values.data_ptr(), ph.data_ptr(), nk, h.data_ptr(), s.data_ptr(), st)
+        return h, s
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            native.library().aosb_bloch_destroy(self.handle)
+            self.handle = None
+
+
+class SymbolicPlan:
+    """Symbolic analysis of one CSR pattern (aosb_plan_create).
+
+    ``ordering="auto"`` analyses the pattern with nested dissection and with
+    the natural order and keeps the one with fewer factorization flops (for
+    3D lattices whose interaction range is long compared with the cell,
+    the banded natural order wins).  Creation is host-only; ``upload`` copies
+    the tables to the device.
+    """
+
+    def __init__(self, n: int, indptr: np.ndarray, indices: np.ndarray, *, tile: int,
+                 supervariables: np.ndarray | None = None, ordering: str = "auto",
+                 device: Any = None, upload: bool = True) -> None:
+        ip = np.ascontiguousarray(indptr, dtype=np.int64)
+        ix = np.ascontiguousarray(indices, dtype=np.int32)
+        sv = None if supervariables is None else np.ascontiguousarray(supervariables, np.int64)
+        modes = {"nested_dissection": [1], "natural": [0], "auto": [1, 0]}[ordering]
+        best = None
+        for mode in modes:
+            opts = native.PlanOptions(native.ABI_VERSION, native.C.sizeof(native.PlanOptions),
+                                      tile, mode, 4 * tile, 1)
+            handle = native.c_vp()
+            native.call("aosb_plan_create", n, ip.ctypes.data, ix.ctypes.data,
+                        None if sv is None else sv.ctypes.data,
+                        0 if sv is None else sv.size - 1, native.C.byref(opts),
+                        native.C.byref(handle))
+            info = native.PlanInfo()
+            native.library().aosb_plan_info(handle, native.C.byref(info))
+            if best is None or info.factor_flops < best[1].factor_flops:
+                if best is not None:
+                    native.library().aosb_plan_destroy(best[0])
+                best = (handle, info, mode)
+            else:
+                native.library().aosb_plan_destroy(handle)
+        self.handle, info, mode = best
+        self.ordering = "nested_dissection" if mode == 1 else "natural"
+        self.info = PlanSummary(info.n, info.n_pad, info.nnz, info.tile, info.n_tiles,
+                                info.n_slots, info.n_nodes, info.tree_levels, info.factor_flops,
+                                info.factor_flops_alg, info.factor_bytes)
+        self.device = device
+        if upload:
+            self.upload()
+
+    def upload(self) -> None:
+        torch = _torch()
+        with torch.cuda.device(self.device):
+            native.call("aosb_plan_upload", self.handle)
+
+    def perm(self) -> np.ndarray:
+        out = np.empty(self.info.n_pad, dtype=np.int32)
+        native.library().aosb_plan_export_perm(self.handle, out.ctypes.data)
+        return out
+
+    def slots(self) -> np.ndarray:
+        nb = self.info.n_tiles
+        out = np.empty(nb * nb, dtype=np.int32)
+        native.library().aosb_plan_export_slots(self.handle, out.ctypes.data)
+        return out.reshape(nb, nb)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            native.library().aosb_plan_destroy(self.handle)
+            self.handle = None
+
+
+@dataclass
+class PencilWork:
+    """One factorization: k row, shift, and the nodes it serves."""
+
+    k: int
+    node: int           # node solved with A = H - z S
+    partner: int | None  # node solved with A^H (conjugate shift), if any
+
+
+def pencil_schedule(n_k: int, shifts: np.ndarray, pair: bool) -> list[PencilWork]:
+    """All (k, node) work items; with ``pair`` node j and node N-1-j share
+    one factorization when z_{N-1-j} == conj(z_j)."""
+    n = shifts.size
+    items: list[PencilWork] = []
+    for k in range(n_k):
+        if pair:
+            for j in range((n + 1) // 2):
+                partner = n - 1 - j
+                close = abs(complex(shifts[partner]) - complex(shifts[j]).conjugate())
+                if partner != j and close <= 1e-5 * max(1.0, abs(complex(shifts[j]))):
+                    items.append(PencilWork(k, j, partner))
+                else:
+                    items.append(PencilWork(k, j, None))
+                    if partner != j:
+                        items.append(PencilWork(k, partner, None))
+        else:
+            items.extend(PencilWork(k, j, None) for j in range(n))
+    return items
+
+
+class BandEngine:
+    """Device-resident Band solver for one bundle."""
+
+    def __init__(self, bundle: LocalizedOperatorBundle, settings: CissSettings | None = None,
+                 engine: EngineSettings | None = None, device: Any = None) -> None:
+        torch = _torch()
+        self.bundle = bundle
+        self.settings = settings or CissSettings()
+        self.engine = engine or EngineSettings()
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None
+                                   else torch.device(device).index or 0)
+        self.n = bundle.n_orbitals
+        if self.settings.search_dimension >= self.n:
+            raise SolverError("CISS search dimension must be smaller than matrix dimension")
+        t0 = perf_counter()
+        self.bloch = BlochDevice(bundle, self.device)
+        self.pattern_seconds = perf_counter() - t0
+        t0 = perf_counter()
+        tile = self.engine.tile or choose_tile(self.n)
+        self.plan = SymbolicPlan(self.n, self.bloch.indptr, self.bloch.indices, tile=tile,
+                                 supervariables=np.asarray(bundle.basis.atom_offsets),
+                                 ordering=self.engine.ordering, device=self.device)
+        self.analysis_seconds = perf_counter() - t0
+        q = probe_block(self.n, self.settings)
+        self.probes = torch.from_numpy(q.astype(np.complex128)).to(self.device)
+        self._gram_scratch = None
+        self.last_stats: dict[str, Any] = {}
+
+    # ------------------------------------------------------------------ utils
+    def _stream(self):
+        torch = _torch()
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _spmm(self, values, x, y) -> None:
+        """y = A x for one k (values [nnz] complex64)."""
+        n, m = x.shape
+        native.call("aosb_spmm", n, m, self.bloch.d_indptr, self.bloch.d_indices,
+                    values.data_ptr(), x.data_ptr(), x.stride(0), y.data_ptr(), y.stride(0),
+                    self._stream())
+
+    def _gram(self, x, y):
+        """x^H y (p x q) in FP64 on the device."""
+        torch = _torch()
+        n, p = x.shape
+        q = y.shape[1]
+        need = native.library().aosb_gram_scratch_bytes(n, p, q)
+        if self._gram_scratch is None or self._gram_scratch.numel() < need:
+            self._gram_scratch = torch.empty(max(need, 16), dtype=torch.uint8, device=self.device)
+        g = torch.empty((p, q), dtype=torch.complex128, device=self.device)
+        native.call("aosb_gram", n, p, q, x.data_ptr(), x.stride(0), y.data_ptr(), y.stride(0),
+                    g.data_ptr(), self._gram_scratch.data_ptr(), self._stream())
+        return g
+
+    def _dense_mul(self, x, t):
+        torch = _torch()
+        n, p = x.shape
+        r = t.shape[1]
+        t = t.contiguous()
+        y = torch.empty((n, r), dtype=torch.complex128, device=self.device)
+        native.call("aosb_dense_mul", n, p, r, x.data_ptr(), x.stride(0), t.data_ptr(),
+                    y.data_ptr(), y.stride(0), self._stream())
+        return y
+
+    def pencil_bytes(self, n_rhs: int) -> int:
+        info = self.plan.info
+        lib = native.library()
+        per = lib.aosb_factor_bytes(self.plan.handle, 1) + 4 * info.n_pad + 4
+        per += 8 * info.n_pad * n_rhs * 2          # normal + adjoint solve blocks (complex64)
+        per += 16 * self.n * n_rhs * 3             # x, r and adjoint x (complex128)
+        return int(per)
+
+    def max_pencils(self, n_rhs: int) -> int:
+        torch = _torch()
+        if self.engine.max_pencils:
+            return self.engine.max_pencils
+        free, _ = torch.cuda.mem_get_info(self.device)
+        budget = int(free * self.engine.memory_fraction)
+        return max(1, min(4096, budget // max(1, self.pencil_bytes(n_rhs))))
+
+    # ------------------------------------------------------------- public API
+    def host_pair(self, k: Sequence[float]) -> SparsePair:
+        """H(k), S(k) as host scipy CSR (for user-supplied solvers)."""
+        from scipy import sparse
+
+        torch = _torch()
+        kp = tuple(float(v) for v in k)
+        if len(kp) != 3:
+            raise InputError("k point must contain three values")
+        h, s = self.bloch.apply(np.asarray([kp]))
+        torch.cuda.synchronize(self.device)
+        hv, sv = h[0].cpu().numpy(), s[0].cpu().numpy()
+        ip = self.bloch.indptr
+        ix = self.bloch.indices
+        if ip[-1] <= np.iinfo(np.int32).max:
+            ip = ip.astype(np.int32)
+        shape = (self.n, self.n)
+        return SparsePair(sparse.csr_matrix((hv, ix, ip), shape=shape, copy=False),
+                          sparse.csr_matrix((sv, ix, ip), shape=shape, copy=False), kp)
+
+    def solve_kpoints(self, kpoints: Sequence[Sequence[float]], interval: EnergyInterval):
+        """CISS for several k points; returns (results, assembly_seconds)."""
+        torch = _torch()
+        if len(kpoints) == 0:
+            return [], []
+        kp = np.asarray([[float(v) for v in k] for k in kpoints], dtype=np.float64)
+        if kp.ndim != 2 or kp.shape[1] != 3:
+            raise InputError("k point must contain three values")
+        with torch.cuda.device(self.device):
+            return self._solve(kp, interval)
+
+    def _solve(self, kp: np.ndarray, interval: EnergyInterval):
+        torch = _torch()
+        st = self.settings
+        mixed = self.engine.precision == "mixed"
+        n, L, M = self.n, st.block_size, st.moment_size
+        nk = kp.shape[0]
+        dev = self.device
+        stages: dict[str, float] = {}
+
+        def tick(name: str, t0: float) -> float:
+            torch.cuda.synchronize(dev)
+            t1 = perf_counter()
+            stages[name] = stages.get(name, 0.0) + (t1 - t0)
+            return t1
+
+        total0 = t = perf_counter()
+        torch.cuda.reset_peak_memory_stats(dev)
+        hvals, svals = self.bloch.apply(kp)
+        t = tick("bloch_assembly", t)
+        assembly = stages["bloch_assembly"] / nk
+        shifts, nodes, weights = contour_geometry(interval, st)
+        coef = moment_coefficients(shifts, nodes, weights, M)
+        rhs = torch.empty((nk, n, L), dtype=torch.complex128, device=dev)
+        for k in range(nk):
+            self._spmm(svals[k], self.probes, rhs[k])
+        mom = torch.zeros((nk, n, L * M), dtype=torch.complex128, device=dev)
+        t = tick("probe_setup", t)
+
+        work = pencil_schedule(nk, shifts, pair=mixed)
+        cap = min(self.max_pencils(L), len(work))
+        info = self.plan.info
+        lib = native.library()
+        precision = (native.PRECISION_BF16X3 if mixed and self.engine.tensor_cores
+                     else native.PRECISION_PLAIN)
+        fbytes = lib.aosb_factor_bytes(self.plan.handle, cap)
+        factor = torch.empty(fbytes // 4, dtype=torch.float32, device=dev)
+        pivots = torch.empty((cap, info.n_pad), dtype=torch.int32, device=dev)
+        status = torch.zeros(cap, dtype=torch.int32, device=dev)
+        wbytes = lib.aosb_factor_workspace_bytes(self.plan.handle, cap, precision)
+        workspace = torch.empty(max(wbytes, 16), dtype=torch.uint8, device=dev)
+        wn = torch.empty((cap, info.n_pad, L), dtype=torch.complex64, device=dev)
+        xn = torch.empty((cap, n, L), dtype=torch.complex128, device=dev)
+        rr = torch.empty((cap, n, L), dtype=torch.complex128, device=dev)
+        coef_d = torch.from_numpy(coef).to(dev)
+        steps = self.engine.refinement_steps if mixed else 0
+        n_factor = 0
+        for b0 in range(0, len(work), cap):
+            batch = work[b0:b0 + cap]
+            np_ = len(batch)
+            pk = torch.tensor([w.k for w in batch], dtype=torch.int32, device=dev)
+            z = torch.from_numpy(shifts[[w.node for w in batch]].astype(np.complex128)).to(dev)
+            status.zero_()
+            fa = native.FactorArgs(native.ABI_VERSION, native.C.sizeof(native.FactorArgs), np_,
+                                   precision, hvals.data_ptr(), svals.data_ptr(), pk.data_ptr(),
+                                   z.data_ptr(), factor.data_ptr(), pivots.data_ptr(),
+                                   status.data_ptr(), workspace.data_ptr(), self._stream())
+            native.call("aosb_factor", self.plan.handle, native.C.byref(fa))
+            n_factor += np_
+            t = tick("native_numeric_factorization", t)
+            bad = status[:np_].cpu().numpy()
+            if np.any(bad != 0):
+                code = int(bad[bad != 0][0])
+                raise SolverError(f"shifted factorization failed with device status {code} "
+                                  f"({native.STATUS_NAMES.get(code, 'unknown')})")
+            # normal solves (node), then adjoint solves (conjugate partner);
+            # a batch without partners skips the adjoint pass
+            for adjoint in (0, 1):
+                if adjoint and all(w.partner is None for w in batch):
+                    continue
+                zz = z if not adjoint else torch.conj_physical(z)
+                self._solve_refined(batch, pk, zz, hvals, svals, rhs, factor, pivots, wn, xn,
+                                    rr, adjoint, steps)
+                t = tick("native_multi_rhs_solve", t)
+                for i, w in enumerate(batch):
+                    node = w.node if adjoint == 0 else w.partner
+                    if node is None:
+                        continue
+                    native.call("aosb_moments_accumulate", n, L, M, xn[i].data_ptr(),
+                                coef_d[node].data_ptr(), mom[w.k].data_ptr(), self._stream())
+                t = tick("moment_accumulation", t)
+        stages["shifted_solves"] = (stages.get("native_numeric_factorization", 0.0)
+                                    + stages.get("native_multi_rhs_solve", 0.0)
+                                    + stages.get("moment_accumulation", 0.0))
+        del factor, pivots, wn, xn, rr, workspace
+        results = []
+        for k in range(nk):
+            results.append(self._subspace(hvals[k], svals[k], mom[k], interval, stages, nk))
+        peak = int(torch.cuda.max_memory_allocated(dev))
+        total = perf_counter() - total0
+        out = []
+        for res in results:
+            res.stage_seconds["solver_total"] = total / nk
+            res.peak_gpu_memory_bytes = peak
+            out.append(res)
+        self.last_stats = {"factorizations": n_factor, "pencil_batch": cap,
+                           "stage_seconds": dict(stages)}
+        return out, [assembly] * nk
+
+    def _solve_refined(self, batch, pk, z, hvals, svals, rhs, factor, pivots, wn, xn, rr,
+                       adjoint: int, steps: int) -> None:
+        """x = A^{-1} b (or A^{-H} b) for every pencil of the batch with
+        ``steps`` FP64 refinement sweeps."""
+        torch = _torch()
+        n, L = self.n, self.settings.block_size
+        np_ = len(batch)
+        st = self._stream()
+        # gather the rhs of each pencil's k into the pencil-major residual buffer
+        kidx = torch.tensor([w.k for w in batch], dtype=torch.long, device=self.device)
+        b = rhs.index_select(0, kidx).contiguous()
+        sa = native.SolveArgs(native.ABI_VERSION, native.C.sizeof(native.SolveArgs), np_, L,
+                              adjoint, 0, factor.data_ptr(), pivots.data_ptr(), wn.data_ptr(), st)
+        for it in range(steps + 1):
+            src = b if it == 0 else rr
+            native.call("aosb_gather_rhs", self.plan.handle, np_, L, src.data_ptr(), n * L,
+                        wn.data_ptr(), st)
+            native.call("aosb_solve", self.plan.handle, native.C.byref(sa))
+            native.call("aosb_scatter_solution", self.plan.handle, np_, L, wn.data_ptr(),
+                        xn.data_ptr(), 1 if it > 0 else 0, st)
+            if it < steps:
+                native.call("aosb_shifted_residual", n, L, np_, self.bloch.d_indptr,
+                            self.bloch.d_indices, hvals.data_ptr(), svals.data_ptr(),
+                            self.bloch.nnz, pk.data_ptr(), z.contiguous().data_ptr(),
+                            b.data_ptr(), n * L, xn.data_ptr(), rr.data_ptr(), st)
+
+    def _subspace(self, h, s, mom, interval: EnergyInterval, stages: dict[str, float],
+                  nk: int) -> CissResult:
+        """Rank truncation, Rayleigh-Ritz, ghost filter and residuals for one k."""
+        torch = _torch()
+        st = self.settings
+        dev = self.device
+        local: dict[str, float] = {k: v / nk for k, v in stages.items()}
+        t = perf_counter()
+        sm = torch.empty_like(mom)
+        self._spmm(s, mom, sm)
+        gram = self._gram(mom, sm).cpu().numpy()
+        transform, sigma = truncate_gram(gram, st.rank_relative_tolerance)
+        basis = self._dense_mul(mom, torch.from_numpy(transform).to(dev))
+        saturated = basis.shape[1] == st.search_dimension
+        torch.cuda.synchronize(dev)
+        local["subspace_compression"] = perf_counter() - t
+        t = perf_counter()
+        hb = torch.empty_like(basis)
+        sb = torch.empty_like(basis)
+        self._spmm(h, basis, hb)
+        self._spmm(s, basis, sb)
+        hr = self._gram(basis, hb).cpu().numpy()
+        sr = self._gram(basis, sb).cpu().numpy()
+        energies, coeffs = projected_eigh(hr, sr)
+        local["rayleigh_ritz"] = perf_counter() - t
+        keep = nonspurious_mask(coeffs, sigma, st.spurious_relative_threshold)
+        inside = (energies > interval.lower_ev) & (energies < interval.upper_ev)
+        sel = np.flatnonzero(keep & inside)
+        max_res = 0.0
+        if sel.size:
+            t = perf_counter()
+            csel = torch.from_numpy(np.ascontiguousarray(coeffs[:, sel])).to(dev)
+            vec = self._dense_mul(basis, csel)
+            hv = torch.empty_like(vec)
+            sv = torch.empty_like(vec)
+            self._spmm(h, vec, hv)
+            self._spmm(s, vec, sv)
+            e_d = torch.from_numpy(np.ascontiguousarray(energies[sel])).to(dev)
+            norms = torch.empty(sel.size, dtype=torch.float64, device=dev)
+            native.call("aosb_column_norms", self.n, int(sel.size), hv.data_ptr(), sv.data_ptr(),
+                        hv.stride(0), e_d.data_ptr(), norms.data_ptr(), self._stream())
+            max_res = float(norms.max().item())
+            local["residual"] = perf_counter() - t
+        selected = np.asarray(energies[sel], dtype=np.float32)
+        return CissResult(selected, max_res, local, None, result_warnings(max_res, saturated),
+                          not saturated)
+
+    def close(self) -> None:
+        self.bloch.close()
+        self.plan.close()

@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Band-path benchmark: k-points/s of mixed-precision batched CISS.
+
+Workload (default ``c2``): seeded synthetic 3D bundle, 1000 atoms x 13
+orbitals (n = 13000, nnz = 15.7M), 121-point Y-G-X-M path, 32 contour
+nodes, 32 probes, 4 moments, a window holding ~100 states at Gamma.  One
+step = the whole Band hot path for ``--kpoints-per-step`` k points:
+device Bloch sums, all shifted factorizations and solves (with FP64
+refinement in mixed precision), moments, Rayleigh-Ritz and FP64 residuals.
+
+Reported (one JSON line on rank 0):
+  value        k-points/s of the chosen form, inputs resident on the GPU
+  e2e          same through BandEngine with the operator block values copied
+               from pinned host memory every step and energies read back
+  plain        k-points/s of the plain complex64 one-node-per-factorization
+               path with no refinement (the drop-in baseline)
+  accuracy     max |E - E_FP64| over sampled k points (FP64 dense oracle)
+  roofline     factorization (dominant, tensor/FP32 bound) achieved TFLOP/s
+  cpu_baseline oracle CISS on the host cores for a bounded sample
+``--impl reference`` times the reference algorithm on the host cores (the
+oracle restatement; the reference's cuDSS extension does not install).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+GUARD_EV = 0.02  # BandCalculation's continuity guard
+
+
+def parse() -> argparse.Namespace:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--kpoints-per-step", type=int, default=0)
+    ap.add_argument("--precision", choices=("mixed", "plain"), default="mixed")
+    ap.add_argument("--tensor-cores", type=int, default=1)
+    ap.add_argument("--plain-kpoints", type=int, default=1)
+    ap.add_argument("--accuracy-kpoints", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        mhz, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def workload(name: str):
+    from aospectrum_b200 import synth
+    from aospectrum_b200.kpath import kpath_from_dict
+
+    w = synth.WORKLOADS[name]
+    return w, kpath_from_dict(w.kpath)
+
+
+def cpu_baseline(bundle, kpts, lo, hi, w, seconds_cap: float = 30.0) -> dict:
+    """Oracle CISS on the host cores: reference Bloch restatement for one k
+    plus one complex64 dense-LU shifted solve (LAPACK, all host threads);
+    k-points/s extrapolated to the N solves a k point needs."""
+    from oracle import bloch_ref, ciss_ref
+    from scipy import sparse
+
+    cores = len(os.sched_getaffinity(0))
+    t0 = time.perf_counter()
+    pat = bloch_ref.build_pattern(bundle)
+    t_pattern = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    h, s = bloch_ref.bloch_pair(pat, bundle, kpts[0])
+    t_bloch = time.perf_counter() - t0
+    n = bundle.n_orbitals
+    hm = sparse.csr_matrix((h, pat.indices, pat.indptr), shape=(n, n))
+    sm = sparse.csr_matrix((s, pat.indices, pat.indptr), shape=(n, n))
+    shifts, nodes, weights = ciss_ref.contour(lo, hi, w.integration_points)
+    q = ciss_ref.probes(n, w.block_size)
+    rhs = np.asarray(sm @ q, dtype=np.complex64)
+    t0 = time.perf_counter()
+    ciss_ref.shifted_solve(hm, sm, shifts[0], rhs, method="dense")
+    t_solve = time.perf_counter() - t0
+    per_k = t_bloch + w.integration_points * t_solve
+    return {"value": 1.0 / per_k, "unit": "k-points/s", "cores": cores, "kind": "port",
+            "sample": (f"oracle Bloch sum of 1 k point ({t_bloch:.2f} s) + 1 of "
+                       f"{w.integration_points} complex64 dense-LU shifted solves "
+                       f"({t_solve:.2f} s, n={n}, {w.block_size} rhs); k-points/s = "
+                       f"1/(t_bloch + {w.integration_points} t_solve); pattern build "
+                       f"{t_pattern:.2f} s once")}
+
+
+def reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w, kp = workload(args.workload)
+    from aospectrum_b200 import synth
+
+    bundle = synth.generate_bundle(w.spec)
+    lo, hi = w.window_ev[0] - GUARD_EV, w.window_ev[1] + GUARD_EV
+    kpts = kp.fractional_points
+    times = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        base = cpu_baseline(bundle, [kpts[i % len(kpts)]], lo, hi, w)
+        if i >= args.warmup:
+            times.append(1.0 / base["value"])
+    per_k = float(np.mean(times))
+    value = 1.0 / per_k
+    out = {"metric": "k-points/s (Band CISS, host reference algorithm)", "value": value,
+           "unit": "k-points/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": per_k * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+           "config": {"workload": f"{w.name}: {w.notes}", "n": w.spec.n_orbitals,
+                      "integration_points": w.integration_points, "block_size": w.block_size,
+                      "moment_size": w.moment_size},
+           "cpu_baseline": {**base, "value": value},
+           "e2e": {"value": value, "unit": "k-points/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main() -> None:
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    from aospectrum_b200 import native, synth
+    from aospectrum_b200.ciss import CissSettings, EngineSettings
+    from aospectrum_b200.data import EnergyInterval
+    from aospectrum_b200.engine import BandEngine
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=dev)
+    w, kp = workload(args.workload)
+    bundle = synth.generate_bundle(w.spec)
+    interval = EnergyInterval(w.window_ev[0] - GUARD_EV, w.window_ev[1] + GUARD_EV)
+    settings = CissSettings(integration_points=w.integration_points, block_size=w.block_size,
+                            moment_size=w.moment_size)
+    eng = BandEngine(bundle, settings,
+                     EngineSettings(precision=args.precision,
+                                    tensor_cores=bool(args.tensor_cores)), device=dev)
+    kpts = kp.fractional_points
+    nk_step = args.kpoints_per_step or (1 if w.spec.n_orbitals > 4000 else 8)
+
+    def kset(step: int) -> np.ndarray:
+        # weak scaling: rank r owns k indices r, r+N, ...; each step takes nk_step of them
+        mine = kpts[rank::world]
+        idx = [(step * nk_step + j) % len(mine) for j in range(nk_step)]
+        return mine[idx]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for i in range(args.warmup):
+        eng.solve_kpoints(kset(i), interval)
+    torch.cuda.synchronize(dev)
+    launches0 = native.library().aosb_launch_count()
+    eng.profile_factor = True
+    eng.factor_times_ms = []
+    barrier()
+    torch.cuda.synchronize(dev)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record()
+        results = []
+        for i in range(args.steps):
+            res, _ = eng.solve_kpoints(kset(args.warmup + i), interval)
+            results.append(res)
+        stop.record()
+        torch.cuda.synchronize(dev)
+    barrier()
+    elapsed = start.elapsed_time(stop) / 1e3
+    launches = native.library().aosb_launch_count() - launches0
+    eng.profile_factor = False
+    t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed = float(t.item())
+    total_k = world * args.steps * nk_step
+    value = total_k / elapsed
+    stats = dict(eng.last_stats)
+    info = eng.plan.info
+    # roofline of the factorization (the dominant kernel group)
+    ft = eng.factor_times_ms
+    per_pencil_flops = info.factor_flops_alg
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (
+        ROOT / "MEASURED_PEAKS.json").exists() else {}
+    tc = args.precision == "mixed" and bool(args.tensor_cores)
+    if tc:
+        peak = peaks.get("bf16_tflops_sustained", 1400.0) / 3.0
+        peak_note = "measured sustained bf16 / 3 (split-BF16 needs 3 products)"
+    else:
+        peak = 74.4
+        peak_note = "nominal FP32 SIMT 148 SM x 128 lanes x 2 x 1.965 GHz (no measured FP32 peak)"
+    if ft:
+        pencils = stats.get("pencil_batch", 1)
+        achieved = per_pencil_flops * np.mean([p for p in eng.factor_pencils]) / (
+            np.mean(ft) / 1e3) / 1e12
+    else:
+        achieved = None
+    roofline = {"bound": "tensor" if tc else "fp32-simt", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
+                "traffic": None, "kernel": "tile LU factorization (schur-dominated)",
+                "peak_source": peak_note,
+                "flops_per_factorization": per_pencil_flops}
+    out = {
+        "metric": "k-points/s at <=1e-4 eV vs FP64 (mixed+batched CISS, 1 B200)",
+        "value": value, "unit": "k-points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": ("c64+bf16x3 tensor-core updates, fp64 refinement" if tc else
+                  ("c64 fp32 updates, fp64 refinement" if args.precision == "mixed" else "c64")),
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": f"{w.name}: {w.notes}", "n": w.spec.n_orbitals, "nnz": info.nnz,
+                   "kpoints_per_step": nk_step, "integration_points": w.integration_points,
+                   "block_size": w.block_size, "moment_size": w.moment_size,
+                   "window_ev": list(w.window_ev), "precision": args.precision,
+                   "tile": info.tile, "ordering": eng.plan.ordering,
+                   "factorizations_per_step": stats.get("factorizations"),
+                   "pencil_batch": stats.get("pencil_batch"),
+                   "l2": "inputs larger than L2 (factor storage %.2f GB per pencil)" % (
+                       info.factor_bytes / 1e9),
+                   "parallelism": f"dp{world} (k points sharded)"},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "roofline": roofline,
+    }
+    if rank == 0:
+        out["stage_seconds_last_step"] = {k: round(v, 4) for k, v in
+                                          stats.get("stage_seconds", {}).items()}
+        # accuracy vs FP64 dense generalized eigenvalues (sampled k points)
+        errs = []
+        for i in range(min(args.accuracy_kpoints, len(kpts))):
+            kpt = kpts[(i * 37) % len(kpts)]
+            res, _ = eng.solve_kpoints([kpt], interval)
+            pair = eng.host_pair(kpt)
+            exact = fp64_window(pair, interval, dev)
+            got = np.sort(res[0].energies_ev.astype(np.float64))
+            if got.size != exact.size:
+                errs.append(float("inf"))
+            else:
+                errs.append(float(np.max(np.abs(got - exact))) if got.size else 0.0)
+        out["accuracy"] = {"max_eig_error_ev": max(errs) if errs else None,
+                           "kpoints_checked": len(errs),
+                           "max_residual_ev": max(r.maximum_residual_ev for rs in results
+                                                  for r in rs),
+                           "oracle": "FP64 dense generalized eigh (torch, cuSOLVER) of the "
+                                     "same H(k), S(k)"}
+        # plain complex64 per-shift baseline on the same GPU
+        if args.plain_kpoints > 0 and args.precision == "mixed":
+            plain = BandEngine(bundle, settings, EngineSettings(precision="plain"), device=dev)
+            plain.solve_kpoints(kset(0)[:1], interval)
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            for i in range(args.plain_kpoints):
+                plain.solve_kpoints(kset(1 + i)[:1], interval)
+            torch.cuda.synchronize(dev)
+            tp = (time.perf_counter() - t0) / args.plain_kpoints
+            plain.close()
+            out["plain"] = {"value": 1.0 / tp, "unit": "k-points/s",
+                            "note": "complex64, one factorization per node, no refinement"}
+            out["speedup_vs_plain"] = value / world / (1.0 / tp)
+        # end to end through the public engine API with host buffers
+        if not args.no_e2e:
+            out["e2e"] = e2e_leg(eng, bundle, kset, interval, args)
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(bundle, [kpts[0]], interval.lower_ev,
+                                               interval.upper_ev, w)
+        print(json.dumps(out), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def fp64_window(pair, interval, dev) -> np.ndarray:
+    import torch
+
+    n = pair.n_orbitals
+    hd = torch.from_numpy(pair.hamiltonian.toarray().astype(np.complex128)).to(dev)
+    sd = torch.from_numpy(pair.overlap.toarray().astype(np.complex128)).to(dev)
+    hd = 0.5 * (hd + hd.conj().T)
+    sd = 0.5 * (sd + sd.conj().T)
+    lc = torch.linalg.cholesky(sd)
+    linv = torch.linalg.solve_triangular(lc, torch.eye(n, dtype=hd.dtype, device=dev),
+                                         upper=False)
+    e = torch.linalg.eigvalsh(linv @ hd @ linv.conj().T).cpu().numpy()
+    del hd, sd, lc, linv
+    torch.cuda.empty_cache()
+    return np.sort(e[(e > interval.lower_ev) & (e < interval.upper_ev)])
+
+
+def e2e_leg(eng, bundle, kset, interval, args) -> dict:
+    """Public-API path with host buffers: every step copies the bundle's
+    block values from pinned host memory into the engine and reads the
+    energies back."""
+    import torch
+
+    hv = torch.from_numpy(np.array(bundle.operators.h_values)).pin_memory()
+    sv = torch.from_numpy(np.array(bundle.operators.s_values)).pin_memory()
+    steps = max(1, args.steps)
+    eng.load_values(hv, sv)
+    eng.solve_kpoints(kset(0), interval)
+    torch.cuda.synchronize()
+    d2h = 0
+    t0 = time.perf_counter()
+    for i in range(steps):
+        eng.load_values(hv, sv)
+        res, _ = eng.solve_kpoints(kset(i), interval)
+        d2h += sum(r.energies_ev.nbytes for r in res)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    nk = len(kset(0))
+    return {"value": nk / dt, "unit": "k-points/s",
+            "h2d_bytes_per_step": int(hv.numel() * hv.element_size() + sv.numel() *
+                                      sv.element_size()),
+            "d2h_bytes_per_step": int(d2h / steps),
+            "path": "BandEngine.load_values (pinned host) + solve_kpoints"}
+
+
+if __name__ == "__main__":
+    main()

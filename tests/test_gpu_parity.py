@@ -1,0 +1,268 @@
+"""GPU parity: every CUDA entry point against the oracle / golden vectors.
+
+Tolerances: the Bloch sum is bit-exact (real block values; complex values
+within 2 ulp); shifted solves match complex128 SuperLU to 2e-4 relative
+(plain complex64 factor, no refinement) or 1e-9 (FP64 refinement); CISS
+eigenvalues match the reference's own CISS and the FP64 dense oracle to
+1e-4 eV.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import json
+
+import numpy as np
+import pytest
+
+import bundles
+from oracle import bloch_ref, dense_ref
+from oracle import ciss_ref
+
+pytestmark = pytest.mark.gpu
+
+EIG_TOL_EV = 1e-4
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+
+    return t
+
+
+def _bloch(bundle, torch):
+    from aospectrum_b200.engine import BlochDevice
+
+    return BlochDevice(bundle, torch.device("cuda", 0))
+
+
+@pytest.mark.parametrize("name", ["tiny2d", "tiny3d", "tinycx"])
+def test_bloch_matches_reference_golden(name, golden, torch):
+    b = bundles.complexified(bundles.tiny2d()) if name == "tinycx" else getattr(bundles, name)()
+    ref = np.load(golden / f"bloch_{name}.npz")
+    dev = _bloch(b, torch)
+    try:
+        assert np.array_equal(dev.indptr, ref["indptr"])
+        assert np.array_equal(dev.indices, ref["indices"])
+        h, s = dev.apply(np.asarray(bundles.KPOINTS))
+        h, s = h.cpu().numpy(), s.cpu().numpy()
+        for i in range(len(bundles.KPOINTS)):
+            if name == "tinycx":
+                # complex block values: products may round differently from numpy's loop
+                np.testing.assert_allclose(h[i], ref[f"h{i}"], rtol=0, atol=2e-6)
+                np.testing.assert_allclose(s[i], ref[f"s{i}"], rtol=0, atol=2e-7)
+            else:
+                assert np.array_equal(h[i], ref[f"h{i}"]), f"H(k{i}) differs"
+                assert np.array_equal(s[i], ref[f"s{i}"]), f"S(k{i}) differs"
+    finally:
+        dev.close()
+
+
+def test_bloch_c1_digest(golden, torch):
+    man = json.loads((golden / "manifest.json").read_text())["bloch"]["c1"]
+    dev = _bloch(bundles.c1(), torch)
+    try:
+        assert dev.nnz == man["nnz"]
+        h, s = dev.apply(np.asarray(bundles.KPOINTS))
+        h, s = h.cpu().numpy(), s.cpu().numpy()
+        for i in range(len(bundles.KPOINTS)):
+            assert _sha(h[i]) == man[f"h{i}"]
+            assert _sha(s[i]) == man[f"s{i}"]
+    finally:
+        dev.close()
+
+
+def _pencil_case(bundle, k, torch, tile, ordering="nested_dissection"):
+    from aospectrum_b200.engine import BlochDevice, SymbolicPlan
+
+    dev = BlochDevice(bundle, torch.device("cuda", 0))
+    plan = SymbolicPlan(dev.n, dev.indptr, dev.indices, tile=tile,
+                        supervariables=np.asarray(bundle.basis.atom_offsets),
+                        ordering=ordering, device=torch.device("cuda", 0))
+    h, s = dev.apply(np.asarray([k]))
+    return dev, plan, h, s
+
+
+def _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=0, adjoint=0, steps=0):
+    """Factor len(shifts) pencils of one k and solve with rhs (n x L)."""
+    from aospectrum_b200 import native
+
+    n, L = rhs.shape
+    P = len(shifts)
+    info = plan.info
+    lib = native.library()
+    dv = torch.device("cuda", 0)
+    factor = torch.empty(lib.aosb_factor_bytes(plan.handle, P) // 4, dtype=torch.float32,
+                         device=dv)
+    piv = torch.empty((P, info.n_pad), dtype=torch.int32, device=dv)
+    status = torch.zeros(P, dtype=torch.int32, device=dv)
+    ws = torch.empty(max(16, lib.aosb_factor_workspace_bytes(plan.handle, P, precision)),
+                     dtype=torch.uint8, device=dv)
+    pk = torch.zeros(P, dtype=torch.int32, device=dv)
+    z = torch.tensor(np.asarray(shifts, dtype=np.complex128), device=dv)
+    st = torch.cuda.current_stream().cuda_stream
+    fa = native.FactorArgs(native.ABI_VERSION, native.C.sizeof(native.FactorArgs), P, precision,
+                           h.data_ptr(), s.data_ptr(), pk.data_ptr(), z.data_ptr(),
+                           factor.data_ptr(), piv.data_ptr(), status.data_ptr(), ws.data_ptr(), st)
+    native.call("aosb_factor", plan.handle, native.C.byref(fa))
+    torch.cuda.synchronize()
+    assert status.cpu().numpy().tolist() == [0] * P
+    b = torch.tensor(np.broadcast_to(rhs, (P, n, L)).astype(np.complex128).copy(), device=dv)
+    x = torch.zeros((P, n, L), dtype=torch.complex128, device=dv)
+    r = torch.zeros_like(x)
+    w = torch.empty((P, info.n_pad, L), dtype=torch.complex64, device=dv)
+    sa = native.SolveArgs(native.ABI_VERSION, native.C.sizeof(native.SolveArgs), P, L, adjoint, 0,
+                          factor.data_ptr(), piv.data_ptr(), w.data_ptr(), st)
+    zz = torch.conj_physical(z) if adjoint else z
+    for it in range(steps + 1):
+        src = b if it == 0 else r
+        native.call("aosb_gather_rhs", plan.handle, P, L, src.data_ptr(), n * L, w.data_ptr(), st)
+        native.call("aosb_solve", plan.handle, native.C.byref(sa))
+        native.call("aosb_scatter_solution", plan.handle, P, L, w.data_ptr(), x.data_ptr(),
+                    1 if it else 0, st)
+        if it < steps:
+            native.call("aosb_shifted_residual", n, L, P, dev.d_indptr, dev.d_indices,
+                        h.data_ptr(), s.data_ptr(), dev.nnz, pk.data_ptr(), zz.data_ptr(),
+                        b.data_ptr(), n * L, x.data_ptr(), r.data_ptr(), st)
+    torch.cuda.synchronize()
+    return x.cpu().numpy()
+
+
+def _splu_reference(dev, h, s, z, rhs, adjoint=False):
+    from scipy import sparse
+    from scipy.sparse import linalg as spl
+
+    n = dev.n
+    hm = sparse.csr_matrix((h[0].cpu().numpy().astype(np.complex128), dev.indices, dev.indptr),
+                           shape=(n, n))
+    sm = sparse.csr_matrix((s[0].cpu().numpy().astype(np.complex128), dev.indices, dev.indptr),
+                           shape=(n, n))
+    zz = np.conj(z) if adjoint else z
+    return spl.splu((hm - zz * sm).tocsc()).solve(rhs.astype(np.complex128))
+
+
+@pytest.mark.parametrize("case,tile,ordering", [("tiny3d", 32, "nested_dissection"),
+                                                ("tiny3d", 32, "natural"),
+                                                ("small2d", 64, "nested_dissection"),
+                                                ("small2d", 128, "nested_dissection")])
+def test_plain_factor_solve_matches_superlu(case, tile, ordering, torch):
+    b = getattr(bundles, case)()
+    dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[1], torch, tile, ordering)
+    try:
+        rng = np.random.default_rng(1)
+        rhs = (rng.standard_normal((dev.n, 8)) + 1j * rng.standard_normal((dev.n, 8)))
+        shifts = [-2.3 + 0.01j, -2.0 + 0.2j, 0.5 + 0.001j]
+        x = _factor_solve(dev, plan, h, s, shifts, rhs, torch)
+        for p, z in enumerate(shifts):
+            ref = _splu_reference(dev, h, s, z, rhs)
+            err = np.linalg.norm(x[p] - ref) / np.linalg.norm(ref)
+            assert err < 2e-4, (p, err)
+    finally:
+        dev.close()
+        plan.close()
+
+
+@pytest.mark.parametrize("adjoint", [0, 1])
+def test_refined_solve_reaches_fp64(adjoint, torch):
+    b = bundles.small2d()
+    dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[2], torch, 64)
+    try:
+        rng = np.random.default_rng(2)
+        rhs = (rng.standard_normal((dev.n, 16)) + 1j * rng.standard_normal((dev.n, 16)))
+        shifts = [-2.25 + 0.003j, -1.95 + 0.03j]
+        x = _factor_solve(dev, plan, h, s, shifts, rhs, torch, adjoint=adjoint, steps=3)
+        for p, z in enumerate(shifts):
+            ref = _splu_reference(dev, h, s, z, rhs, adjoint=bool(adjoint))
+            err = np.linalg.norm(x[p] - ref) / np.linalg.norm(ref)
+            assert err < 1e-9, (p, err)
+    finally:
+        dev.close()
+        plan.close()
+
+
+def test_ubatch_dropin_host_buffers(torch):
+    """aospectrum_b200_solve_complex64_ubatch_v1 with the reference's packing
+    (values = H - z S per batch entry, column-major rhs)."""
+    from aospectrum_b200 import native
+
+    b = bundles.tiny3d()
+    dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[3], torch, 32)
+    try:
+        n, nnz, B, L = dev.n, dev.nnz, 3, 5
+        hv, sv = h[0].cpu().numpy(), s[0].cpu().numpy()
+        shifts = np.asarray([-2.0 + 0.05j, -1.0 + 0.01j, 0.3 + 0.4j], dtype=np.complex64)
+        values = np.stack([hv - z * sv for z in shifts]).astype(np.complex64)
+        rng = np.random.default_rng(4)
+        rhs = (rng.standard_normal((B, L, n)) + 1j * rng.standard_normal((B, L, n))).astype(
+            np.complex64)
+        sol = np.zeros_like(rhs)
+        ip = dev.indptr.astype(np.int32)
+        req = native.UbatchRequest(native.ABI_VERSION, native.C.sizeof(native.UbatchRequest), n,
+                                   nnz, B, L, ip.ctypes.data, dev.indices.ctypes.data,
+                                   values.ctypes.data, rhs.ctypes.data, sol.ctypes.data)
+        res = native.UbatchResult()
+        rc = native.library().aospectrum_b200_solve_complex64_ubatch_v1(native.C.byref(req),
+                                                                       native.C.byref(res))
+        assert rc == 0 and res.status == 0, res.error_message
+        assert res.iterative_refinement_steps == 2
+        from scipy import sparse
+        from scipy.sparse import linalg as spl
+
+        for bi in range(B):
+            a = sparse.csr_matrix((values[bi].astype(np.complex128), dev.indices, dev.indptr),
+                                  shape=(n, n))
+            ref = spl.splu(a.tocsc()).solve(rhs[bi].T.astype(np.complex128))
+            err = np.linalg.norm(sol[bi].T - ref) / np.linalg.norm(ref)
+            assert err < 1e-6, err
+        # error path: a non-finite value is rejected with status 35
+        values[1, 3] = np.nan
+        res2 = native.UbatchResult()
+        rc = native.library().aospectrum_b200_solve_complex64_ubatch_v1(native.C.byref(req),
+                                                                       native.C.byref(res2))
+        assert rc != 0 and res2.status == 35
+    finally:
+        dev.close()
+        plan.close()
+
+
+def _engine(bundle, precision, tensor_cores=True, **kw):
+    from aospectrum_b200.ciss import CissSettings, EngineSettings
+    from aospectrum_b200.engine import BandEngine
+
+    return BandEngine(bundle, CissSettings(**kw),
+                      EngineSettings(precision=precision, tensor_cores=tensor_cores))
+
+
+@pytest.mark.parametrize("precision,tc", [("plain", False), ("mixed", False)])
+@pytest.mark.parametrize("key", ["tiny3d_k2", "small2d_k2", "tinycx_k1", "c1_k0"])
+def test_engine_ciss_matches_reference(key, precision, tc, golden, torch):
+    from aospectrum_b200.data import EnergyInterval
+
+    case = json.loads((golden / "manifest.json").read_text())["ciss"][key]
+    ref_e = np.load(golden / "ciss.npz")[f"{key}_energies"]
+    name = case["bundle"]
+    b = bundles.complexified(bundles.tiny2d()) if name == "tinycx" else getattr(bundles, name)()
+    eng = _engine(b, precision, tc, integration_points=case["integration_points"],
+                  block_size=case["block_size"], moment_size=case["moment_size"])
+    try:
+        lo, hi = case["interval"]
+        res, _ = eng.solve_kpoints([bundles.KPOINTS[case["k_index"]]], EnergyInterval(lo, hi))
+        got = np.sort(res[0].energies_ev.astype(np.float64))
+        assert got.size == ref_e.size, (got, ref_e)
+        assert np.max(np.abs(got - np.sort(ref_e))) < EIG_TOL_EV
+        # FP64 dense oracle
+        pair = eng.host_pair(bundles.KPOINTS[case["k_index"]])
+        hd, sd = dense_ref.dense_pair(pair.hamiltonian.indptr, pair.hamiltonian.indices,
+                                      pair.hamiltonian.data, pair.overlap.data, eng.n)
+        exact = dense_ref.window(dense_ref.eigenvalues(hd, sd), lo, hi)
+        assert exact.size == got.size
+        assert np.max(np.abs(got - exact)) < EIG_TOL_EV
+        # residual no worse than the reference's complex64 CISS
+        assert res[0].maximum_residual_ev <= max(case["max_residual_ev"], 1e-6) * 1.01
+    finally:
+        eng.close()
