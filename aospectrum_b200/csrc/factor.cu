@@ -329,31 +329,47 @@ __global__ void __launch_bounds__(kThreads) schur_kernel(int nU, const int32_t* 
 }
 
 template <int T>
-int run_plain(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
+int ensure_diag_attr(char* err, size_t cap) {
+  static bool done = false;
+  if (done) return 0;
+  const size_t diag_smem = (size_t)(2 * T * T + 2 * T) * sizeof(float) + T * sizeof(int);
+  cudaError_t e = cudaFuncSetAttribute(diag_lu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)diag_smem);
+  if (e != cudaSuccess)
+    return set_error(err, cap, AOSB_ERR_CUDA, "diag_lu smem attribute: %s", cudaGetErrorString(e));
+  done = true;
+  return 0;
+}
+
+// Diagonal LU and panel updates of step k (FP32 SIMT).
+template <int T>
+void step_panels(const aosb_plan* P, const aosb_factor_args_v1* a, int64_t k) {
   cudaStream_t st = (cudaStream_t)a->stream;
   const int np = a->n_pencils;
   const size_t diag_smem = (size_t)(2 * T * T + 2 * T) * sizeof(float) + T * sizeof(int);
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(diag_lu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)diag_smem);
-    if (e != cudaSuccess)
-      return set_error(err, cap, AOSB_ERR_CUDA, "diag_lu smem attribute: %s", cudaGetErrorString(e));
-    attr_done = true;
-  }
-  for (int64_t k = 0; k < P->nb; ++k) {
-    diag_lu_kernel<T><<<np, kThreads, diag_smem, st>>>((int)k, P->d_diag_slot, P->n_slots, P->n_pad,
-                                                      a->factor, a->pivots, a->status);
+  diag_lu_kernel<T><<<np, kThreads, diag_smem, st>>>((int)k, P->d_diag_slot, P->n_slots, P->n_pad,
+                                                    a->factor, a->pivots, a->status);
+  count_launches(1);
+  const int nL = P->lb_off[k + 1] - P->lb_off[k];
+  const int nU = P->ur_off[k + 1] - P->ur_off[k];
+  if (nL + nU > 0) {
+    dim3 grid((unsigned)((nL + nU) * PanelCfg<T>::kStrips), np);
+    panel_kernel<T><<<grid, kThreads, 0, st>>>((int)k, nL, nU, P->d_lb_slot + P->lb_off[k],
+                                               P->d_ur_slot + P->ur_off[k], P->d_diag_slot,
+                                               P->n_slots, P->n_pad, a->factor, a->pivots);
     count_launches(1);
+  }
+}
+
+template <int T>
+int run_plain(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
+  cudaStream_t st = (cudaStream_t)a->stream;
+  const int np = a->n_pencils;
+  if (int rc = ensure_diag_attr<T>(err, cap)) return rc;
+  for (int64_t k = 0; k < P->nb; ++k) {
+    step_panels<T>(P, a, k);
     const int nL = P->lb_off[k + 1] - P->lb_off[k];
     const int nU = P->ur_off[k + 1] - P->ur_off[k];
-    if (nL + nU > 0) {
-      dim3 grid((unsigned)((nL + nU) * PanelCfg<T>::kStrips), np);
-      panel_kernel<T><<<grid, kThreads, 0, st>>>((int)k, nL, nU, P->d_lb_slot + P->lb_off[k],
-                                                 P->d_ur_slot + P->ur_off[k], P->d_diag_slot,
-                                                 P->n_slots, P->n_pad, a->factor, a->pivots);
-      count_launches(1);
-    }
     if (nL > 0 && nU > 0) {
       const int64_t blocks = (int64_t)nL * nU * SchurCfg<T>::kSub;
       if (blocks > INT32_MAX) return set_error(err, cap, AOSB_ERR_SIZE, "schur grid too large");
@@ -384,6 +400,16 @@ int factor_assemble(const aosb_plan* P, const aosb_factor_args_v1* a, char* err,
                                           (int)P->T, a->factor);
   count_launches(2);
   return launch_check(err, cap, "assemble");
+}
+
+int factor_step_panels(const aosb_plan* P, const aosb_factor_args_v1* a, int k, char* err,
+                       size_t cap) {
+  switch (P->T) {
+    case 32: if (int rc = ensure_diag_attr<32>(err, cap)) return rc; step_panels<32>(P, a, k); return 0;
+    case 64: if (int rc = ensure_diag_attr<64>(err, cap)) return rc; step_panels<64>(P, a, k); return 0;
+    case 128: if (int rc = ensure_diag_attr<128>(err, cap)) return rc; step_panels<128>(P, a, k); return 0;
+  }
+  return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "unsupported tile size");
 }
 
 int factor_plain(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {

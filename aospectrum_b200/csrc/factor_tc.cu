@@ -1,18 +1,389 @@
 // Tensor-core (tcgen05) factorization path: split-BF16 Schur updates.
+//
+// Same right-looking tile LU as factor.cu (diagonal LU and panels stay FP32
+// SIMT); the Schur update A_ij -= L_ik U_kj of every step runs on the 5th
+// generation tensor cores:
+//
+//   * stage_kernel converts the step's L tiles (i,k) and U tiles (k,j) into
+//     four BF16 planes each -- re_hi, re_lo, im_hi, im_lo with
+//     x = hi + lo, hi = bf16(x), lo = bf16(x - hi) -- laid out as UMMA
+//     K-major, no-swizzle core matrices (8 rows x 16 bytes), cut into 16-wide
+//     K slabs so that one slab of one tile is a single contiguous bulk copy.
+//     For U the operand rows are U's columns (B is K-major).
+//   * schur_tc_kernel: one CTA (4 warps) per (target tile, pencil).  Lane 0
+//     of warp 0 streams slabs with cp.async.bulk into a 3-stage mbarrier
+//     ring; lane 0 of warp 1 issues, per 16-wide K step, 12
+//     tcgen05.mma.kind::f16 (M=128, N=128) into two FP32 TMEM accumulators:
+//       Re += Lr_h Ur_h + Lr_h Ur_l + Lr_l Ur_h - (Li_h Ui_h + Li_h Ui_l + Li_l Ui_h)
+//       Im += Lr_h Ui_h + Lr_h Ui_l + Lr_l Ui_h + Li_h Ur_h + Li_h Ur_l + Li_l Ur_h
+//     (the minus via the instruction's negate-A bit; lo*lo is dropped).
+//     All four warps then read the accumulators with tcgen05.ld and apply
+//     C -= acc to the FP32 tile in HBM.
+//   Every mbarrier wait is bounded; on expiry the CTA records
+//   AOSB_ERR_TIMEOUT in the pencil status, skips the remaining work, and
+//   still frees its TMEM.
+#include "plan.h"
 #include "factor.h"
+#include "cgemm.cuh"
+
+#include <cuda_bf16.h>
 
 namespace aosb {
+namespace {
+
+constexpr int kTcT = 128;                 // tile edge supported by this path
+constexpr int kSlabK = 16;                // K per slab (one MMA K step)
+constexpr int kSlabs = kTcT / kSlabK;     // 8
+constexpr int kPlaneSlabBytes = kTcT * kSlabK * 2;          // 4096
+constexpr int kOperandSlabBytes = 4 * kPlaneSlabBytes;      // 16384
+constexpr int kStagedTileBytes = kSlabs * kOperandSlabBytes;  // 131072
+constexpr int kStages = 3;
+constexpr int kTcThreads = 128;
+constexpr uint32_t kTmemCols = 256;
+constexpr long long kWaitLimit = 1ll << 22;  // polls (with backoff) before timeout
+
+__device__ __forceinline__ size_t tile_base(int64_t p, int64_t n_slots, int64_t slot) {
+  return ((size_t)p * (size_t)n_slots + (size_t)slot) * (size_t)(2 * kTcT * kTcT);
+}
+
+// Byte offset of operand element (row, k) of plane `plane` in a staged tile.
+__host__ __device__ __forceinline__ uint32_t staged_offset(int row, int k, int plane) {
+  const int slab = k / kSlabK, kk = k % kSlabK;
+  return (uint32_t)(slab * kOperandSlabBytes + plane * kPlaneSlabBytes +
+                    (kk / 8) * ((kTcT / 8) * 128) + (row / 8) * 128 + (row % 8) * 16 +
+                    (kk % 8) * 2);
+}
+
+// ---------------------------------------------------------------------------
+// Staging: blockIdx.x = item (L tiles first, then U tiles), blockIdx.y = pencil.
+__global__ void __launch_bounds__(256) stage_kernel(int nL, int nU, const int32_t* __restrict__ lslot,
+                                                    const int32_t* __restrict__ uslot,
+                                                    int64_t n_slots, const float* __restrict__ factor,
+                                                    unsigned char* __restrict__ staging,
+                                                    int64_t staging_pencil_stride) {
+  const int item = blockIdx.x, p = blockIdx.y;
+  const bool is_l = item < nL;
+  const int slot = is_l ? lslot[item] : uslot[item - nL];
+  const float* F = factor + tile_base(p, n_slots, slot);
+  unsigned char* out = staging + (size_t)p * staging_pencil_stride + (size_t)item * kStagedTileBytes;
+  // Each thread converts pairs of consecutive k for one operand row, so a
+  // 4-byte store writes two BF16 values.
+  for (int e = threadIdx.x; e < kTcT * (kTcT / 2); e += blockDim.x) {
+    int row, k;
+    float r0, i0, r1, i1;
+    if (is_l) {
+      // A = L (row-major): operand row = tile row, k = tile column
+      row = e / (kTcT / 2);
+      k = (e % (kTcT / 2)) * 2;
+      const size_t o = (size_t)row * kTcT + k;
+      r0 = F[o]; r1 = F[o + 1];
+      i0 = F[o + kTcT * kTcT]; i1 = F[o + 1 + kTcT * kTcT];
+    } else {
+      // B = U (row-major, k x n): operand row = column n, k = tile row
+      k = (e / kTcT) * 2;
+      row = e % kTcT;
+      const size_t o0 = (size_t)k * kTcT + row, o1 = (size_t)(k + 1) * kTcT + row;
+      r0 = F[o0]; r1 = F[o1];
+      i0 = F[o0 + kTcT * kTcT]; i1 = F[o1 + kTcT * kTcT];
+    }
+    const float re[2] = {r0, r1}, im[2] = {i0, i1};
+    __nv_bfloat162 plane[4];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const __nv_bfloat16 rh = __float2bfloat16_rn(re[t]);
+      const __nv_bfloat16 rl = __float2bfloat16_rn(re[t] - __bfloat162float(rh));
+      const __nv_bfloat16 ih = __float2bfloat16_rn(im[t]);
+      const __nv_bfloat16 il = __float2bfloat16_rn(im[t] - __bfloat162float(ih));
+      if (t == 0) {
+        plane[0].x = rh; plane[1].x = rl; plane[2].x = ih; plane[3].x = il;
+      } else {
+        plane[0].y = rh; plane[1].y = rl; plane[2].y = ih; plane[3].y = il;
+      }
+    }
+#pragma unroll
+    for (int pl = 0; pl < 4; ++pl)
+      *reinterpret_cast<__nv_bfloat162*>(out + staged_offset(row, k, pl)) = plane[pl];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PTX helpers.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// Bounded wait on phase `parity`; returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  for (long long it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (it > 64) __nanosleep(128);
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version (Blackwell)
+  return d;               // base offset 0, lbo mode 0, layout SWIZZLE_NONE (0)
+}
+
+// Instruction descriptor: BF16 x BF16 -> F32, K-major A and B, M = N = 128.
+__host__ __device__ constexpr uint32_t umma_idesc(bool negate_a) {
+  return (1u << 4)                    // D format F32
+         | (1u << 7)                  // A format BF16
+         | (1u << 10)                 // B format BF16
+         | ((negate_a ? 1u : 0u) << 13)
+         | ((uint32_t)(kTcT >> 3) << 17)   // N / 8
+         | ((uint32_t)(kTcT >> 4) << 24);  // M / 16
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+struct TcShared {
+  alignas(1024) unsigned char a[kStages][kOperandSlabBytes];
+  alignas(1024) unsigned char b[kStages][kOperandSlabBytes];
+  uint64_t full[kStages];
+  uint64_t empty[kStages];
+  uint64_t done;
+  uint32_t tmem_base;
+  int failed;
+};
+
+__global__ void __launch_bounds__(kTcThreads) schur_tc_kernel(
+    int nU, int step_items, const int32_t* __restrict__ tslot, int64_t n_slots,
+    float* __restrict__ factor, const unsigned char* __restrict__ staging,
+    int64_t staging_pencil_stride, int32_t* __restrict__ status) {
+  extern __shared__ unsigned char dyn[];
+  TcShared& sh = *reinterpret_cast<TcShared*>(
+      (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int pair = blockIdx.x, p = blockIdx.y;
+  const int a = pair / nU, b = pair % nU;
+  const unsigned char* stA = staging + (size_t)p * staging_pencil_stride + (size_t)a * kStagedTileBytes;
+  const unsigned char* stB =
+      staging + (size_t)p * staging_pencil_stride + (size_t)(step_items + b) * kStagedTileBytes;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&sh.full[s], 1);
+      mbar_init(&sh.empty[s], 1);
+    }
+    mbar_init(&sh.done, 1);
+    sh.failed = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&sh.tmem_base)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = sh.tmem_base;
+
+  if (warp == 0 && lane == 0) {
+    // Producer: one 16 KB bulk copy per operand per slab.
+    for (int s = 0; s < kSlabs; ++s) {
+      const int st = s % kStages;
+      if (s >= kStages && !mbar_wait(&sh.empty[st], ((s / kStages) - 1) & 1)) {
+        sh.failed = 1;
+        break;
+      }
+      mbar_expect_tx(&sh.full[st], 2 * kOperandSlabBytes);
+      bulk_g2s(sh.a[st], stA + (size_t)s * kOperandSlabBytes, kOperandSlabBytes, &sh.full[st]);
+      bulk_g2s(sh.b[st], stB + (size_t)s * kOperandSlabBytes, kOperandSlabBytes, &sh.full[st]);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer.
+    const uint32_t id_pos = umma_idesc(false), id_neg = umma_idesc(true);
+    const uint32_t lbo = (kTcT / 8) * 128, sbo = 128;
+    bool ok = true;
+    for (int s = 0; s < kSlabs && ok; ++s) {
+      const int st = s % kStages;
+      if (!mbar_wait(&sh.full[st], (s / kStages) & 1)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t sa = smem_u32(sh.a[st]), sb = smem_u32(sh.b[st]);
+      // planes: 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo
+      uint64_t A[4], Bv[4];
+#pragma unroll
+      for (int pl = 0; pl < 4; ++pl) {
+        A[pl] = umma_desc(sa + pl * kPlaneSlabBytes, lbo, sbo);
+        Bv[pl] = umma_desc(sb + pl * kPlaneSlabBytes, lbo, sbo);
+      }
+      const uint32_t re = tmem, im = tmem + kTcT;
+      const uint32_t first = s == 0 ? 0u : 1u;
+      umma_bf16(re, A[0], Bv[0], id_pos, first);
+      umma_bf16(re, A[0], Bv[1], id_pos, 1);
+      umma_bf16(re, A[1], Bv[0], id_pos, 1);
+      umma_bf16(re, A[2], Bv[2], id_neg, 1);
+      umma_bf16(re, A[2], Bv[3], id_neg, 1);
+      umma_bf16(re, A[3], Bv[2], id_neg, 1);
+      umma_bf16(im, A[0], Bv[2], id_pos, first);
+      umma_bf16(im, A[0], Bv[3], id_pos, 1);
+      umma_bf16(im, A[1], Bv[2], id_pos, 1);
+      umma_bf16(im, A[2], Bv[0], id_pos, 1);
+      umma_bf16(im, A[2], Bv[1], id_pos, 1);
+      umma_bf16(im, A[3], Bv[0], id_pos, 1);
+      umma_commit(&sh.empty[st]);  // frees this stage when its MMAs finish
+    }
+    if (ok) umma_commit(&sh.done);
+    else sh.failed = 1;
+  }
+  __syncwarp();
+  // Epilogue: warp w owns accumulator rows (TMEM lanes) 32w .. 32w+31.
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.done, 0) ? 1 : 0) != 0;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    float* C = factor + tile_base(p, n_slots, tslot[pair]);
+    const int row = warp * 32 + lane;
+    const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
+#pragma unroll 1
+    for (int c0 = 0; c0 < kTcT; c0 += 16) {
+      float vr[16], vi[16];
+      tmem_ld16(tmem + lane_addr + c0, vr);
+      tmem_ld16(tmem + lane_addr + kTcT + c0, vi);
+      float4* cr = reinterpret_cast<float4*>(C + (size_t)row * kTcT + c0);
+      float4* ci = reinterpret_cast<float4*>(C + kTcT * kTcT + (size_t)row * kTcT + c0);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float4 x = cr[q], y = ci[q];
+        x.x -= vr[4 * q]; x.y -= vr[4 * q + 1]; x.z -= vr[4 * q + 2]; x.w -= vr[4 * q + 3];
+        y.x -= vi[4 * q]; y.y -= vi[4 * q + 1]; y.z -= vi[4 * q + 2]; y.w -= vi[4 * q + 3];
+        cr[q] = x;
+        ci[q] = y;
+      }
+    }
+  }
+  if (!ok || sh.failed) {
+    if (threadIdx.x == 0) atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols));
+  }
+}
+
+}  // namespace
 
 size_t factor_tc_workspace(const aosb_plan* P, int32_t n_pencils) {
-  (void)P;
-  (void)n_pencils;
-  return 0;
+  if (P->T != kTcT) return 0;
+  int64_t most = 0;
+  for (int64_t k = 0; k < P->nb; ++k) {
+    const int64_t items = (P->lb_off[k + 1] - P->lb_off[k]) + (P->ur_off[k + 1] - P->ur_off[k]);
+    most = items > most ? items : most;
+  }
+  return (size_t)(most > 0 ? most : 1) * kStagedTileBytes * (size_t)n_pencils;
 }
 
 int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
-  (void)P;
-  (void)a;
-  return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "tensor-core path not built");
+  if (P->T != kTcT)
+    return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "tensor-core path needs tile = 128");
+  if (a->workspace == nullptr)
+    return set_error(err, cap, AOSB_ERR_NULL, "tensor-core path needs a staging workspace");
+  cudaStream_t st = (cudaStream_t)a->stream;
+  const int np = a->n_pencils;
+  // The full 227 KB keeps every address a descriptor can form inside this
+  // CTA's shared memory.
+  const size_t smem = 232448;
+  static_assert(sizeof(TcShared) + 1024 <= 232448, "shared memory budget");
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(schur_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess)
+      return set_error(err, cap, AOSB_ERR_CUDA, "schur_tc smem attribute: %s", cudaGetErrorString(e));
+    attr_done = true;
+  }
+  int64_t most = 0;
+  for (int64_t k = 0; k < P->nb; ++k) {
+    const int64_t items = (P->lb_off[k + 1] - P->lb_off[k]) + (P->ur_off[k + 1] - P->ur_off[k]);
+    most = items > most ? items : most;
+  }
+  const int64_t pencil_stride = (most > 0 ? most : 1) * (int64_t)kStagedTileBytes;
+  unsigned char* staging = (unsigned char*)a->workspace;
+  for (int64_t k = 0; k < P->nb; ++k) {
+    int rc = factor_step_panels(P, a, (int)k, err, cap);
+    if (rc) return rc;
+    const int nL = P->lb_off[k + 1] - P->lb_off[k];
+    const int nU = P->ur_off[k + 1] - P->ur_off[k];
+    if (nL == 0 || nU == 0) continue;
+    stage_kernel<<<dim3(nL + nU, np), 256, 0, st>>>(nL, nU, P->d_lb_slot + P->lb_off[k],
+                                                   P->d_ur_slot + P->ur_off[k], P->n_slots,
+                                                   a->factor, staging, pencil_stride);
+    const int64_t pairs = (int64_t)nL * nU;
+    schur_tc_kernel<<<dim3((unsigned)pairs, np), kTcThreads, smem, st>>>(
+        nU, nL, P->d_sc_slot + P->sc_off[k], P->n_slots, a->factor, staging, pencil_stride,
+        a->status);
+    count_launches(2);
+  }
+  return launch_check(err, cap, "tensor-core factorization");
 }
 
 }  // namespace aosb

@@ -262,7 +262,8 @@ class BandEngine:
         self.bloch = BlochDevice(bundle, self.device)
         self.pattern_seconds = perf_counter() - t0
         t0 = perf_counter()
-        tile = self.engine.tile or choose_tile(self.n)
+        use_tc = self.engine.precision == "mixed" and self.engine.tensor_cores
+        tile = self.engine.tile or (128 if use_tc else choose_tile(self.n))
         self.plan = SymbolicPlan(self.n, self.bloch.indptr, self.bloch.indices, tile=tile,
                                  supervariables=np.asarray(bundle.basis.atom_offsets),
                                  ordering=self.engine.ordering, device=self.device)
@@ -271,6 +272,10 @@ class BandEngine:
         self.probes = torch.from_numpy(q.astype(np.complex128)).to(self.device)
         self._gram_scratch = None
         self.last_stats: dict[str, Any] = {}
+        # optional device timing of every factorization call (CUDA events)
+        self.profile_factor = False
+        self.factor_times_ms: list[float] = []
+        self.factor_pencils: list[int] = []
 
     # ------------------------------------------------------------------ utils
     def _stream(self):
@@ -324,6 +329,16 @@ class BandEngine:
         return max(1, min(4096, budget // max(1, self.pencil_bytes(n_rhs))))
 
     # ------------------------------------------------------------- public API
+    def load_values(self, h_values, s_values) -> None:
+        """Replace the resident block values (same pattern) from host
+        tensors/arrays; pinned host memory gives an asynchronous copy."""
+        torch = _torch()
+        for dst, src in ((self.bloch.h_values, h_values), (self.bloch.s_values, s_values)):
+            t = src if isinstance(src, torch.Tensor) else torch.from_numpy(np.asarray(src))
+            if t.numel() != dst.numel():
+                raise InputError("block values do not match the bundle pattern")
+            dst.copy_(t.reshape(dst.shape).to(dst.dtype), non_blocking=True)
+
     def host_pair(self, k: Sequence[float]) -> SparsePair:
         """H(k), S(k) as host scipy CSR (for user-supplied solvers)."""
         from scipy import sparse
@@ -410,7 +425,16 @@ class BandEngine:
                                    precision, hvals.data_ptr(), svals.data_ptr(), pk.data_ptr(),
                                    z.data_ptr(), factor.data_ptr(), pivots.data_ptr(),
                                    status.data_ptr(), workspace.data_ptr(), self._stream())
+            if self.profile_factor:
+                ev0 = torch.cuda.Event(enable_timing=True)
+                ev1 = torch.cuda.Event(enable_timing=True)
+                ev0.record()
             native.call("aosb_factor", self.plan.handle, native.C.byref(fa))
+            if self.profile_factor:
+                ev1.record()
+                ev1.synchronize()
+                self.factor_times_ms.append(ev0.elapsed_time(ev1))
+                self.factor_pencils.append(np_)
             n_factor += np_
             t = tick("native_numeric_factorization", t)
             bad = status[:np_].cpu().numpy()

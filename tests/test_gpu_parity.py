@@ -167,6 +167,32 @@ def test_plain_factor_solve_matches_superlu(case, tile, ordering, torch):
         plan.close()
 
 
+@pytest.mark.parametrize("case", ["small2d", "c1"])
+def test_tensor_core_factor_matches_superlu(case, torch):
+    """Split-BF16 tcgen05 Schur updates: unrefined solves within 1e-3, FP64
+    refinement to 1e-9, both directions."""
+    b = getattr(bundles, case)()
+    dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[1], torch, 128)
+    try:
+        rng = np.random.default_rng(3)
+        rhs = (rng.standard_normal((dev.n, 8)) + 1j * rng.standard_normal((dev.n, 8)))
+        shifts = [-2.6 + 0.004j, -2.4 + 0.04j, -1.0 + 0.5j]
+        x0 = _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=1)
+        for adjoint in (0, 1):
+            x = _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=1, adjoint=adjoint,
+                              steps=3)
+            for p, z in enumerate(shifts):
+                ref = _splu_reference(dev, h, s, z, rhs, adjoint=bool(adjoint))
+                if adjoint == 0:
+                    e0 = np.linalg.norm(x0[p] - ref) / np.linalg.norm(ref)
+                    assert e0 < 1e-3, (p, e0)
+                err = np.linalg.norm(x[p] - ref) / np.linalg.norm(ref)
+                assert err < 1e-9, (adjoint, p, err)
+    finally:
+        dev.close()
+        plan.close()
+
+
 @pytest.mark.parametrize("adjoint", [0, 1])
 def test_refined_solve_reaches_fp64(adjoint, torch):
     b = bundles.small2d()
@@ -238,7 +264,7 @@ def _engine(bundle, precision, tensor_cores=True, **kw):
                       EngineSettings(precision=precision, tensor_cores=tensor_cores))
 
 
-@pytest.mark.parametrize("precision,tc", [("plain", False), ("mixed", False)])
+@pytest.mark.parametrize("precision,tc", [("plain", False), ("mixed", False), ("mixed", True)])
 @pytest.mark.parametrize("key", ["tiny3d_k2", "small2d_k2", "tinycx_k1", "c1_k0"])
 def test_engine_ciss_matches_reference(key, precision, tc, golden, torch):
     from aospectrum_b200.data import EnergyInterval
