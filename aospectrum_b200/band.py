@@ -97,6 +97,8 @@ class BandCalculation:
     settings: CissSettings = field(default_factory=CissSettings)
     solver: Any | None = None
     engine_settings: EngineSettings = field(default_factory=EngineSettings)
+    engine_factory: Any | None = None
+    lazy_engine: bool = False
     solve_interval_ev: EnergyInterval = field(init=False)
     absolute_interval_ev: EnergyInterval = field(init=False)
     engine: Any = field(init=False)
@@ -108,9 +110,9 @@ class BandCalculation:
         self.absolute_interval_ev = EnergyInterval(
             self.solve_interval_ev.lower_ev + ref, self.solve_interval_ev.upper_ev + ref
         )
-        from .engine import BandEngine
-
-        self.engine = BandEngine(self.bundle, self.settings, self.engine_settings)
+        self.engine = None
+        if not self.lazy_engine:
+            self.engine = self._make_engine()
         notes = []
         if self.bundle.basis.spinor_width != 1:
             notes.append("spinor input is outside the current non-SOC Band scope; "
@@ -119,6 +121,13 @@ class BandCalculation:
             notes.append("non-periodic axes are outside the current Bloch scope; "
                          "the result may be inaccurate")
         self.warnings = tuple(notes)
+
+    def _make_engine(self):
+        if self.engine_factory is not None:
+            return self.engine_factory(self.bundle, self.settings, self.engine_settings)
+        from .engine import BandEngine
+
+        return BandEngine(self.bundle, self.settings, self.engine_settings)
 
     def _check_index(self, index: int) -> int:
         if not 0 <= int(index) < self.kpath.n_points:
@@ -133,6 +142,8 @@ class BandCalculation:
         factorizations when memory allows."""
         idx = [self._check_index(i) for i in indices]
         kpts = [self.kpath.fractional_points[i] for i in idx]
+        if self.engine is None:
+            self.engine = self._make_engine()
         if self.solver is None:
             results, assembly = self.engine.solve_kpoints(kpts, self.absolute_interval_ev)
         else:
@@ -164,7 +175,8 @@ class BandCalculation:
         closer = getattr(self.solver, "close", None)
         if callable(closer):
             closer()
-        self.engine.close()
+        if self.engine is not None:
+            self.engine.close()
 
 
 def write_point(path: str | Path, point: BandPoint) -> None:

@@ -209,12 +209,14 @@ int aospectrum_b200_solve_complex64_ubatch_v1(const aospectrum_b200_ubatch_reque
   float2* d_work = nullptr;
   float* d_factor = nullptr;
   int32_t *d_piv = nullptr, *d_status = nullptr, *d_pk = nullptr;
+  void* d_solve_scratch = nullptr;
   double2* d_shift = nullptr;
   int rc = 0;
   auto cleanup = [&]() {
     cudaFree(d_vals); cudaFree(d_rhs_cm); cudaFree(d_b); cudaFree(d_x); cudaFree(d_r);
     cudaFree(d_work); cudaFree(d_factor); cudaFree(d_piv); cudaFree(d_status); cudaFree(d_pk);
     cudaFree(d_shift);
+    cudaFree(d_solve_scratch);
     if (st) cudaStreamDestroy(st);
   };
   auto cuda_ok = [&](cudaError_t e, const char* what) {
@@ -237,6 +239,7 @@ int aospectrum_b200_solve_complex64_ubatch_v1(const aospectrum_b200_ubatch_reque
       !cuda_ok(cudaMalloc(&d_status, sizeof(int32_t) * B), "status") ||
       !cuda_ok(cudaMalloc(&d_pk, sizeof(int32_t) * B), "pencil index") ||
       !cuda_ok(cudaMalloc(&d_shift, sizeof(double2) * B), "shifts") ||
+      !cuda_ok(cudaMalloc(&d_solve_scratch, aosb_solve_scratch_bytes(plan, B, L)), "solve scratch") ||
       !cuda_ok(cudaMemcpyAsync(d_vals, req->values, sizeof(float2) * (size_t)B * nnz,
                                cudaMemcpyHostToDevice, st), "values upload") ||
       !cuda_ok(cudaMemcpyAsync(d_rhs_cm, req->rhs, sizeof(float2) * B * nL,
@@ -287,7 +290,7 @@ int aospectrum_b200_solve_complex64_ubatch_v1(const aospectrum_b200_ubatch_reque
   // solve -> x += work; r = b - A x}.
   const double ts = now_seconds();
   aosb_solve_args_v1 sa{AOSPECTRUM_B200_ABI_VERSION, sizeof(aosb_solve_args_v1), B, L, 0, 0,
-                        d_factor, d_piv, (aosb_complex64*)d_work, st};
+                        d_factor, d_piv, (aosb_complex64*)d_work, d_solve_scratch, st};
   const int steps = res->iterative_refinement_steps;
   for (int it = 0; it <= steps && rc == 0; ++it) {
     const double2* src = it == 0 ? d_b : d_r;

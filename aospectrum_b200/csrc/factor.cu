@@ -70,37 +70,52 @@ __global__ void pad_identity_kernel(int64_t n_pad, const int32_t* __restrict__ p
 
 // ---------------------------------------------------------------------------
 // Diagonal tile: LU with partial pivoting in shared memory + triangle inverses.
+// Rows are padded to T+1 floats so that walking a column touches 32
+// different banks; 512 threads.
+constexpr int kDiagThreads = 512;
+
 template <int T>
-__global__ void __launch_bounds__(kThreads) diag_lu_kernel(int k, const int32_t* __restrict__ diag_slot,
-                                                           int64_t n_slots, int64_t n_pad,
-                                                           float* __restrict__ factor,
-                                                           int32_t* __restrict__ pivots,
-                                                           int32_t* __restrict__ status) {
+constexpr size_t diag_smem_bytes() {
+  // tile (2 planes, padded rows) + scratch column (2T) + perm (T) + the
+  // recursive-inverse temporaries (2 planes of T*T/2)
+  return (size_t)(2 * T * (T + 1) + 2 * T) * sizeof(float) + T * sizeof(int) +
+         (size_t)T * T * sizeof(float);
+}
+
+template <int T>
+__global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(int k, const int32_t* __restrict__ diag_slot,
+                                                               int64_t n_slots, int64_t n_pad,
+                                                               float* __restrict__ factor,
+                                                               int32_t* __restrict__ pivots,
+                                                               int32_t* __restrict__ status) {
+  constexpr int LD = T + 1;
   extern __shared__ float smem[];
-  float* ar = smem;              // T*T
-  float* ai = smem + T * T;      // T*T
-  float* colr = ai + T * T;      // T  (scratch column)
-  float* coli = colr + T;        // T
-  int* perm = (int*)(coli + T);  // T
+  float* ar = smem;               // T x LD
+  float* ai = smem + T * LD;      // T x LD
+  float* colr = ai + T * LD;      // T  (scratch column)
+  float* coli = colr + T;         // T
+  int* perm = (int*)(coli + T);   // T
   __shared__ int s_piv;
   __shared__ float s_pr, s_pi;
   const int p = blockIdx.x;
   const int tid = threadIdx.x;
   float* g = factor + tile_base(p, n_slots, diag_slot[k], T);
-  for (int e = tid; e < T * T; e += kThreads) {
-    ar[e] = g[e];
-    ai[e] = g[e + T * T];
+  for (int e = tid; e < T * T; e += kDiagThreads) {
+    const int r = e / T, c = e % T;  // T is a power of two
+    ar[r * LD + c] = g[e];
+    ai[r * LD + c] = g[e + T * T];
   }
-  for (int r = tid; r < T; r += kThreads) perm[r] = r;
+  for (int r = tid; r < T; r += kDiagThreads) perm[r] = r;
   __syncthreads();
   int bad = 0;
+  // 2D thread layout for the rank-1 update: 16 row lanes x 32 column lanes.
+  const int ty = tid / 32, tx = tid % 32;
   for (int j = 0; j < T; ++j) {
-    // Pivot search by warp 0.
     if (tid < 32) {
       float best = -1.0f;
       int bi = j;
       for (int r = j + tid; r < T; r += 32) {
-        const float m = fabsf(ar[r * T + j]) + fabsf(ai[r * T + j]);
+        const float m = fabsf(ar[r * LD + j]) + fabsf(ai[r * LD + j]);
         if (m > best) { best = m; bi = r; }
       }
 #pragma unroll
@@ -109,91 +124,181 @@ __global__ void __launch_bounds__(kThreads) diag_lu_kernel(int k, const int32_t*
         const int oi = __shfl_down_sync(0xffffffffu, bi, o);
         if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
       }
-      if (tid == 0) s_piv = bi;
+      if (tid == 0) {
+        s_piv = bi;
+        float pr = ar[bi * LD + j], pi = ai[bi * LD + j];
+        float d = pr * pr + pi * pi;
+        if (!(d > 0.0f) || !isfinite(d)) {
+          bad = isfinite(d) ? kDevZeroPivot : kDevNonFinite;
+          pr = 1.0f; pi = 0.0f; d = 1.0f;
+        }
+        s_pr = pr / d;
+        s_pi = -pi / d;
+      }
     }
     __syncthreads();
     const int pv = s_piv;
     if (pv != j) {
-      for (int c = tid; c < T; c += kThreads) {
-        float t = ar[j * T + c]; ar[j * T + c] = ar[pv * T + c]; ar[pv * T + c] = t;
-        t = ai[j * T + c]; ai[j * T + c] = ai[pv * T + c]; ai[pv * T + c] = t;
+      for (int c = tid; c < T; c += kDiagThreads) {
+        float t = ar[j * LD + c]; ar[j * LD + c] = ar[pv * LD + c]; ar[pv * LD + c] = t;
+        t = ai[j * LD + c]; ai[j * LD + c] = ai[pv * LD + c]; ai[pv * LD + c] = t;
       }
       if (tid == 0) { int t = perm[j]; perm[j] = perm[pv]; perm[pv] = t; }
+      __syncthreads();
     }
-    __syncthreads();
-    if (tid == 0) {
-      float pr = ar[j * T + j], pi = ai[j * T + j];
-      float d = pr * pr + pi * pi;
-      if (!(d > 0.0f) || !isfinite(d)) {
-        bad = isfinite(d) ? kDevZeroPivot : kDevNonFinite;
-        pr = 1.0f; pi = 0.0f; d = 1.0f;
-        ar[j * T + j] = 1.0f; ai[j * T + j] = 0.0f;
-      }
-      s_pr = pr / d;
-      s_pi = -pi / d;
-    }
-    __syncthreads();
+    if (tid == 0 && bad) { ar[j * LD + j] = 1.0f; ai[j * LD + j] = 0.0f; }
     const float ipr = s_pr, ipi = s_pi;
-    for (int r = j + 1 + tid; r < T; r += kThreads) {
-      const float xr = ar[r * T + j], xi = ai[r * T + j];
-      ar[r * T + j] = xr * ipr - xi * ipi;
-      ai[r * T + j] = xr * ipi + xi * ipr;
+    // scale the column below the pivot
+    for (int r = j + 1 + tid; r < T; r += kDiagThreads) {
+      const float xr = ar[r * LD + j], xi = ai[r * LD + j];
+      ar[r * LD + j] = xr * ipr - xi * ipi;
+      ai[r * LD + j] = xr * ipi + xi * ipr;
     }
     __syncthreads();
-    const int m = T - j - 1;
-    for (int e = tid; e < m * m; e += kThreads) {
-      const int r = j + 1 + e / m, c = j + 1 + e % m;
-      const float lr = ar[r * T + j], li = ai[r * T + j];
-      const float ur = ar[j * T + c], ui = ai[j * T + c];
-      ar[r * T + c] -= lr * ur - li * ui;
-      ai[r * T + c] -= lr * ui + li * ur;
+    // rank-1 update of the trailing block
+    for (int r = j + 1 + ty; r < T; r += kDiagThreads / 32) {
+      const float lr = ar[r * LD + j], li = ai[r * LD + j];
+      for (int c = j + 1 + tx; c < T; c += 32) {
+        const float ur = ar[j * LD + c], ui = ai[j * LD + c];
+        ar[r * LD + c] -= lr * ur - li * ui;
+        ai[r * LD + c] -= lr * ui + li * ur;
+      }
     }
     __syncthreads();
   }
-  // inv(U): columns left to right; column j of the inverse needs the
-  // already inverted leading block and the original column j.
-  for (int j = 0; j < T; ++j) {
-    for (int r = tid; r <= j; r += kThreads) { colr[r] = ar[r * T + j]; coli[r] = ai[r * T + j]; }
-    __syncthreads();
-    // d = 1 / u_jj
-    const float ur = colr[j], ui = coli[j];
-    const float dd = ur * ur + ui * ui;
-    const float dr = ur / dd, di = -ui / dd;
-    for (int i = tid; i < j; i += kThreads) {
+  // Triangle inverses by recursive 2x2 blocking: invert the 8x8 diagonal
+  // blocks (one warp each), then for b = 8, 16, ... , T/2 combine adjacent
+  // blocks:  X12 = -X11 U12 X22  (upper)  and  X21 = -X22 L21 X11  (unit
+  // lower).  tr/ti hold the b x b temporaries of all pairs of a level.
+  float* tr = colr + 2 * T + T;   // after perm (see diag_smem_bytes)
+  float* ti = tr + T * T / 2;
+  const int warp = tid / 32, lane = tid % 32;
+  // ---- base: 8x8 diagonal blocks, warp w < T/8 takes block w
+  if (warp < T / 8) {
+    const int b0 = warp * 8;
+    const int i = lane % 8;
+    // upper, non-unit: column by column, lane i = row
+    for (int j = 0; j < 8; ++j) {
+      float cr[8], ci[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        cr[q] = ar[(b0 + q) * LD + b0 + j];
+        ci[q] = ai[(b0 + q) * LD + b0 + j];
+      }
+      __syncwarp();
+      const float dd = cr[j] * cr[j] + ci[j] * ci[j];
+      const float dr = cr[j] / dd, di = -ci[j] / dd;
+      if (lane < 8 && i <= j) {
+        if (i == j) {
+          ar[(b0 + j) * LD + b0 + j] = dr;
+          ai[(b0 + j) * LD + b0 + j] = di;
+        } else {
+          float sr = 0.0f, si = 0.0f;
+          for (int q = i; q < j; ++q) {
+            const float xr = ar[(b0 + i) * LD + b0 + q], xi = ai[(b0 + i) * LD + b0 + q];
+            sr += xr * cr[q] - xi * ci[q];
+            si += xr * ci[q] + xi * cr[q];
+          }
+          ar[(b0 + i) * LD + b0 + j] = -(sr * dr - si * di);
+          ai[(b0 + i) * LD + b0 + j] = -(sr * di + si * dr);
+        }
+      }
+      __syncwarp();
+    }
+    // unit lower: columns right to left
+    for (int j = 6; j >= 0; --j) {
+      float cr[8], ci[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        cr[q] = ar[(b0 + q) * LD + b0 + j];
+        ci[q] = ai[(b0 + q) * LD + b0 + j];
+      }
+      __syncwarp();
+      if (lane < 8 && i > j) {
+        float sr = cr[i], si = ci[i];
+        for (int q = j + 1; q < i; ++q) {
+          const float xr = ar[(b0 + i) * LD + b0 + q], xi = ai[(b0 + i) * LD + b0 + q];
+          sr += xr * cr[q] - xi * ci[q];
+          si += xr * ci[q] + xi * cr[q];
+        }
+        ar[(b0 + i) * LD + b0 + j] = -sr;
+        ai[(b0 + i) * LD + b0 + j] = -si;
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // ---- combine levels
+  for (int b = 8; b < T; b *= 2) {
+    const int pairs = T / (2 * b);
+    const int per = b * b;
+    // upper: T1 = U12 X22 (X22 upper incl. diagonal)
+    for (int e = tid; e < pairs * per; e += kDiagThreads) {
+      const int m = e / per, r = (e % per) / b, c = e % b;
+      const int A0 = 2 * b * m, B0 = A0 + b;
       float sr = 0.0f, si = 0.0f;
-      for (int q = i; q < j; ++q) {
-        const float xr = ar[i * T + q], xi = ai[i * T + q];
-        sr += xr * colr[q] - xi * coli[q];
-        si += xr * coli[q] + xi * colr[q];
+      for (int q = 0; q <= c; ++q) {
+        const float ur = ar[(A0 + r) * LD + B0 + q], ui = ai[(A0 + r) * LD + B0 + q];
+        const float xr = ar[(B0 + q) * LD + B0 + c], xi = ai[(B0 + q) * LD + B0 + c];
+        sr += ur * xr - ui * xi;
+        si += ur * xi + ui * xr;
       }
-      ar[i * T + j] = -(sr * dr - si * di);
-      ai[i * T + j] = -(sr * di + si * dr);
-    }
-    if (tid == 0) { ar[j * T + j] = dr; ai[j * T + j] = di; }
-    __syncthreads();
-  }
-  // inv(L) (unit lower): columns right to left.
-  for (int j = T - 2; j >= 0; --j) {
-    for (int r = j + 1 + tid; r < T; r += kThreads) { colr[r] = ar[r * T + j]; coli[r] = ai[r * T + j]; }
-    __syncthreads();
-    for (int i = j + 1 + tid; i < T; i += kThreads) {
-      // x_i = l_ij + sum_{q=j+1}^{i-1} Linv[i][q] l_qj
-      float sr = colr[i], si = coli[i];
-      for (int q = j + 1; q < i; ++q) {
-        const float xr = ar[i * T + q], xi = ai[i * T + q];
-        sr += xr * colr[q] - xi * coli[q];
-        si += xr * coli[q] + xi * colr[q];
-      }
-      ar[i * T + j] = -sr;
-      ai[i * T + j] = -si;
+      tr[e] = sr;
+      ti[e] = si;
     }
     __syncthreads();
+    // X12 = -X11 T1 (X11 upper incl. diagonal), written over U12
+    for (int e = tid; e < pairs * per; e += kDiagThreads) {
+      const int m = e / per, r = (e % per) / b, c = e % b;
+      const int A0 = 2 * b * m, B0 = A0 + b;
+      float sr = 0.0f, si = 0.0f;
+      for (int q = r; q < b; ++q) {
+        const float xr = ar[(A0 + r) * LD + A0 + q], xi = ai[(A0 + r) * LD + A0 + q];
+        const float t_r = tr[m * per + q * b + c], t_i = ti[m * per + q * b + c];
+        sr += xr * t_r - xi * t_i;
+        si += xr * t_i + xi * t_r;
+      }
+      ar[(A0 + r) * LD + B0 + c] = -sr;
+      ai[(A0 + r) * LD + B0 + c] = -si;
+    }
+    __syncthreads();
+    // lower: T1 = L21 X11 (X11 unit lower)
+    for (int e = tid; e < pairs * per; e += kDiagThreads) {
+      const int m = e / per, r = (e % per) / b, c = e % b;
+      const int A0 = 2 * b * m, B0 = A0 + b;
+      float sr = ar[(B0 + r) * LD + A0 + c], si = ai[(B0 + r) * LD + A0 + c];
+      for (int q = c + 1; q < b; ++q) {
+        const float lr = ar[(B0 + r) * LD + A0 + q], li = ai[(B0 + r) * LD + A0 + q];
+        const float xr = ar[(A0 + q) * LD + A0 + c], xi = ai[(A0 + q) * LD + A0 + c];
+        sr += lr * xr - li * xi;
+        si += lr * xi + li * xr;
+      }
+      tr[e] = sr;
+      ti[e] = si;
+    }
+    __syncthreads();
+    // X21 = -X22 T1 (X22 unit lower), written over L21
+    for (int e = tid; e < pairs * per; e += kDiagThreads) {
+      const int m = e / per, r = (e % per) / b, c = e % b;
+      const int A0 = 2 * b * m, B0 = A0 + b;
+      float sr = tr[m * per + r * b + c], si = ti[m * per + r * b + c];
+      for (int q = 0; q < r; ++q) {
+        const float xr = ar[(B0 + r) * LD + B0 + q], xi = ai[(B0 + r) * LD + B0 + q];
+        const float t_r = tr[m * per + q * b + c], t_i = ti[m * per + q * b + c];
+        sr += xr * t_r - xi * t_i;
+        si += xr * t_i + xi * t_r;
+      }
+      ar[(B0 + r) * LD + A0 + c] = -sr;
+      ai[(B0 + r) * LD + A0 + c] = -si;
+    }
+    __syncthreads();
   }
-  for (int e = tid; e < T * T; e += kThreads) {
-    g[e] = ar[e];
-    g[e + T * T] = ai[e];
+  for (int e = tid; e < T * T; e += kDiagThreads) {
+    const int r = e / T, c = e % T;
+    g[e] = ar[r * LD + c];
+    g[e + T * T] = ai[r * LD + c];
   }
-  for (int r = tid; r < T; r += kThreads) pivots[(size_t)p * n_pad + (size_t)k * T + r] = perm[r];
+  for (int r = tid; r < T; r += kDiagThreads) pivots[(size_t)p * n_pad + (size_t)k * T + r] = perm[r];
   if (tid == 0 && bad != 0 && status[p] == 0) status[p] = bad;
 }
 
@@ -332,7 +437,7 @@ template <int T>
 int ensure_diag_attr(char* err, size_t cap) {
   static bool done = false;
   if (done) return 0;
-  const size_t diag_smem = (size_t)(2 * T * T + 2 * T) * sizeof(float) + T * sizeof(int);
+  const size_t diag_smem = diag_smem_bytes<T>();
   cudaError_t e = cudaFuncSetAttribute(diag_lu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)diag_smem);
   if (e != cudaSuccess)
@@ -346,8 +451,8 @@ template <int T>
 void step_panels(const aosb_plan* P, const aosb_factor_args_v1* a, int64_t k) {
   cudaStream_t st = (cudaStream_t)a->stream;
   const int np = a->n_pencils;
-  const size_t diag_smem = (size_t)(2 * T * T + 2 * T) * sizeof(float) + T * sizeof(int);
-  diag_lu_kernel<T><<<np, kThreads, diag_smem, st>>>((int)k, P->d_diag_slot, P->n_slots, P->n_pad,
+  const size_t diag_smem = diag_smem_bytes<T>();
+  diag_lu_kernel<T><<<np, kDiagThreads, diag_smem, st>>>((int)k, P->d_diag_slot, P->n_slots, P->n_pad,
                                                     a->factor, a->pivots, a->status);
   count_launches(1);
   const int nL = P->lb_off[k + 1] - P->lb_off[k];

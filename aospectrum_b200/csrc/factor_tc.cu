@@ -37,9 +37,6 @@ constexpr int kSlabs = kTcT / kSlabK;     // 8
 constexpr int kPlaneSlabBytes = kTcT * kSlabK * 2;          // 4096
 constexpr int kOperandSlabBytes = 4 * kPlaneSlabBytes;      // 16384
 constexpr int kStagedTileBytes = kSlabs * kOperandSlabBytes;  // 131072
-constexpr int kStages = 3;
-constexpr int kTcThreads = 128;
-constexpr uint32_t kTmemCols = 256;
 constexpr long long kWaitLimit = 1ll << 22;  // polls (with backoff) before timeout
 
 __device__ __forceinline__ size_t tile_base(int64_t p, int64_t n_slots, int64_t slot) {
@@ -198,43 +195,62 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-struct TcShared {
-  alignas(1024) unsigned char a[kStages][kOperandSlabBytes];
-  alignas(1024) unsigned char b[kStages][kOperandSlabBytes];
-  uint64_t full[kStages];
-  uint64_t empty[kStages];
-  uint64_t done;
+// Persistent, warp-specialized Schur update.  Each CTA (one per SM) walks
+// the step's (pencil, target) items with stride gridDim.x:
+//   warp 8 lane 0  producer: 16-wide K slabs of A (L_ik) and B (U_kj) into a
+//                  kStages-deep ring (cp.async.bulk + mbarrier complete_tx);
+//   warp 9 lane 0  MMA issuer: 12 tcgen05.mma per slab into accumulator set
+//                  acc (TMEM columns acc*256 + [0,128) real, +[128,256) imag);
+//   warps 0-7      epilogue: C rows 32*(w%4) + lane, columns 64*(w/4) ..+63;
+//                  the C values are loaded before the accumulator is ready,
+//                  then C -= acc is stored.
+// Two accumulator sets let the epilogue of one item overlap the MMAs of the
+// next.
+constexpr int kStagesP = 6;
+constexpr int kEpiWarps = 8;
+constexpr int kPThreads = (kEpiWarps + 2) * 32;
+constexpr uint32_t kTmemColsP = 512;
+
+struct PShared {
+  alignas(1024) unsigned char a[kStagesP][kOperandSlabBytes];
+  alignas(1024) unsigned char b[kStagesP][kOperandSlabBytes];
+  uint64_t full[kStagesP];
+  uint64_t empty[kStagesP];
+  uint64_t acc_full[2];
+  uint64_t acc_empty[2];
   uint32_t tmem_base;
   int failed;
 };
 
-__global__ void __launch_bounds__(kTcThreads) schur_tc_kernel(
-    int nU, int step_items, const int32_t* __restrict__ tslot, int64_t n_slots,
-    float* __restrict__ factor, const unsigned char* __restrict__ staging,
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
+    int nU, int step_items, int n_pairs, int n_pencils, const int32_t* __restrict__ tslot,
+    int64_t n_slots, float* __restrict__ factor, const unsigned char* __restrict__ staging,
     int64_t staging_pencil_stride, int32_t* __restrict__ status) {
   extern __shared__ unsigned char dyn[];
-  TcShared& sh = *reinterpret_cast<TcShared*>(
+  PShared& sh = *reinterpret_cast<PShared*>(
       (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int pair = blockIdx.x, p = blockIdx.y;
-  const int a = pair / nU, b = pair % nU;
-  const unsigned char* stA = staging + (size_t)p * staging_pencil_stride + (size_t)a * kStagedTileBytes;
-  const unsigned char* stB =
-      staging + (size_t)p * staging_pencil_stride + (size_t)(step_items + b) * kStagedTileBytes;
-
+  const int total = n_pairs * n_pencils;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < kStagesP; ++s) {
       mbar_init(&sh.full[s], 1);
       mbar_init(&sh.empty[s], 1);
     }
-    mbar_init(&sh.done, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&sh.acc_full[b], 1);
+      mbar_init(&sh.acc_empty[b], kEpiWarps);
+    }
     sh.failed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&sh.tmem_base)),
-                 "r"(kTmemCols));
+                 "r"(kTmemColsP));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -242,91 +258,143 @@ __global__ void __launch_bounds__(kTcThreads) schur_tc_kernel(
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = sh.tmem_base;
 
-  if (warp == 0 && lane == 0) {
-    // Producer: one 16 KB bulk copy per operand per slab.
-    for (int s = 0; s < kSlabs; ++s) {
-      const int st = s % kStages;
-      if (s >= kStages && !mbar_wait(&sh.empty[st], ((s / kStages) - 1) & 1)) {
-        sh.failed = 1;
-        break;
+  if (warp == kEpiWarps) {
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      for (int it = blockIdx.x; it < total && !sh.failed; it += gridDim.x) {
+        const int p = it / n_pairs, pair = it % n_pairs;
+        const unsigned char* stA = staging + (size_t)p * staging_pencil_stride +
+                                   (size_t)(pair / nU) * kStagedTileBytes;
+        const unsigned char* stB = staging + (size_t)p * staging_pencil_stride +
+                                   (size_t)(step_items + pair % nU) * kStagedTileBytes;
+        for (int s = 0; s < kSlabs; ++s) {
+          if (!mbar_wait(&sh.empty[stage], phase ^ 1)) {
+            sh.failed = 1;
+            atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
+            break;
+          }
+          mbar_expect_tx(&sh.full[stage], 2 * kOperandSlabBytes);
+          bulk_g2s(sh.a[stage], stA + (size_t)s * kOperandSlabBytes, kOperandSlabBytes,
+                   &sh.full[stage]);
+          bulk_g2s(sh.b[stage], stB + (size_t)s * kOperandSlabBytes, kOperandSlabBytes,
+                   &sh.full[stage]);
+          if (++stage == kStagesP) { stage = 0; phase ^= 1; }
+        }
       }
-      mbar_expect_tx(&sh.full[st], 2 * kOperandSlabBytes);
-      bulk_g2s(sh.a[st], stA + (size_t)s * kOperandSlabBytes, kOperandSlabBytes, &sh.full[st]);
-      bulk_g2s(sh.b[st], stB + (size_t)s * kOperandSlabBytes, kOperandSlabBytes, &sh.full[st]);
     }
-  } else if (warp == 1 && lane == 0) {
-    // MMA issuer.
-    const uint32_t id_pos = umma_idesc(false), id_neg = umma_idesc(true);
-    const uint32_t lbo = (kTcT / 8) * 128, sbo = 128;
-    bool ok = true;
-    for (int s = 0; s < kSlabs && ok; ++s) {
-      const int st = s % kStages;
-      if (!mbar_wait(&sh.full[st], (s / kStages) & 1)) {
-        ok = false;
+  } else if (warp == kEpiWarps + 1) {
+    if (lane == 0) {
+      const uint32_t id_pos = umma_idesc(false), id_neg = umma_idesc(true);
+      const uint32_t lbo = (kTcT / 8) * 128, sbo = 128;
+      int stage = 0, acc = 0;
+      uint32_t phase = 0, acc_phase = 0;
+      for (int it = blockIdx.x; it < total && !sh.failed; it += gridDim.x) {
+        const int p = it / n_pairs;
+        if (!mbar_wait(&sh.acc_empty[acc], acc_phase ^ 1)) {
+          sh.failed = 1;
+          atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t re = tmem + (uint32_t)acc * 256, im = re + kTcT;
+        bool ok = true;
+        for (int s = 0; s < kSlabs; ++s) {
+          if (!mbar_wait(&sh.full[stage], phase)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t sa = smem_u32(sh.a[stage]), sb = smem_u32(sh.b[stage]);
+          uint64_t A[4], Bv[4];
+#pragma unroll
+          for (int pl = 0; pl < 4; ++pl) {
+            A[pl] = umma_desc(sa + pl * kPlaneSlabBytes, lbo, sbo);
+            Bv[pl] = umma_desc(sb + pl * kPlaneSlabBytes, lbo, sbo);
+          }
+          const uint32_t first = s == 0 ? 0u : 1u;
+          umma_bf16(re, A[0], Bv[0], id_pos, first);
+          umma_bf16(re, A[0], Bv[1], id_pos, 1);
+          umma_bf16(re, A[1], Bv[0], id_pos, 1);
+          umma_bf16(re, A[2], Bv[2], id_neg, 1);
+          umma_bf16(re, A[2], Bv[3], id_neg, 1);
+          umma_bf16(re, A[3], Bv[2], id_neg, 1);
+          umma_bf16(im, A[0], Bv[2], id_pos, first);
+          umma_bf16(im, A[0], Bv[3], id_pos, 1);
+          umma_bf16(im, A[1], Bv[2], id_pos, 1);
+          umma_bf16(im, A[2], Bv[0], id_pos, 1);
+          umma_bf16(im, A[2], Bv[1], id_pos, 1);
+          umma_bf16(im, A[3], Bv[0], id_pos, 1);
+          umma_commit(&sh.empty[stage]);
+          if (++stage == kStagesP) { stage = 0; phase ^= 1; }
+        }
+        if (!ok) {
+          sh.failed = 1;
+          atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
+          break;
+        }
+        umma_commit(&sh.acc_full[acc]);
+        if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+      }
+    }
+  } else {
+    // Epilogue warps.
+    const int quarter = warp % 4, half = warp / 4;
+    const int row = quarter * 32 + lane;
+    const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    for (int it = blockIdx.x; it < total; it += gridDim.x) {
+      const int p = it / n_pairs, pair = it % n_pairs;
+      float* C = factor + tile_base(p, n_slots, tslot[pair]);
+      float4* cr = reinterpret_cast<float4*>(C + (size_t)row * kTcT + half * 64);
+      float4* ci = reinterpret_cast<float4*>(C + kTcT * kTcT + (size_t)row * kTcT + half * 64);
+      float4 xr[16], xi[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        xr[q] = cr[q];
+        xi[q] = ci[q];
+      }
+      const bool ready = __all_sync(0xffffffffu, mbar_wait(&sh.acc_full[acc], acc_phase) ? 1 : 0);
+      if (!ready) {
+        if (lane == 0) {
+          sh.failed = 1;
+          atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
+        }
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t sa = smem_u32(sh.a[st]), sb = smem_u32(sh.b[st]);
-      // planes: 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo
-      uint64_t A[4], Bv[4];
+      const uint32_t base = tmem + (uint32_t)acc * 256 + (uint32_t)half * 64;
 #pragma unroll
-      for (int pl = 0; pl < 4; ++pl) {
-        A[pl] = umma_desc(sa + pl * kPlaneSlabBytes, lbo, sbo);
-        Bv[pl] = umma_desc(sb + pl * kPlaneSlabBytes, lbo, sbo);
-      }
-      const uint32_t re = tmem, im = tmem + kTcT;
-      const uint32_t first = s == 0 ? 0u : 1u;
-      umma_bf16(re, A[0], Bv[0], id_pos, first);
-      umma_bf16(re, A[0], Bv[1], id_pos, 1);
-      umma_bf16(re, A[1], Bv[0], id_pos, 1);
-      umma_bf16(re, A[2], Bv[2], id_neg, 1);
-      umma_bf16(re, A[2], Bv[3], id_neg, 1);
-      umma_bf16(re, A[3], Bv[2], id_neg, 1);
-      umma_bf16(im, A[0], Bv[2], id_pos, first);
-      umma_bf16(im, A[0], Bv[3], id_pos, 1);
-      umma_bf16(im, A[1], Bv[2], id_pos, 1);
-      umma_bf16(im, A[2], Bv[0], id_pos, 1);
-      umma_bf16(im, A[2], Bv[1], id_pos, 1);
-      umma_bf16(im, A[3], Bv[0], id_pos, 1);
-      umma_commit(&sh.empty[st]);  // frees this stage when its MMAs finish
-    }
-    if (ok) umma_commit(&sh.done);
-    else sh.failed = 1;
-  }
-  __syncwarp();
-  // Epilogue: warp w owns accumulator rows (TMEM lanes) 32w .. 32w+31.
-  const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.done, 0) ? 1 : 0) != 0;
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (ok) {
-    float* C = factor + tile_base(p, n_slots, tslot[pair]);
-    const int row = warp * 32 + lane;
-    const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
-#pragma unroll 1
-    for (int c0 = 0; c0 < kTcT; c0 += 16) {
-      float vr[16], vi[16];
-      tmem_ld16(tmem + lane_addr + c0, vr);
-      tmem_ld16(tmem + lane_addr + kTcT + c0, vi);
-      float4* cr = reinterpret_cast<float4*>(C + (size_t)row * kTcT + c0);
-      float4* ci = reinterpret_cast<float4*>(C + kTcT * kTcT + (size_t)row * kTcT + c0);
+      for (int c = 0; c < 4; ++c) {
+        float vr[16], vi[16];
+        tmem_ld16(base + lane_addr + c * 16, vr);
+        tmem_ld16(base + lane_addr + kTcT + c * 16, vi);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        float4 x = cr[q], y = ci[q];
-        x.x -= vr[4 * q]; x.y -= vr[4 * q + 1]; x.z -= vr[4 * q + 2]; x.w -= vr[4 * q + 3];
-        y.x -= vi[4 * q]; y.y -= vi[4 * q + 1]; y.z -= vi[4 * q + 2]; y.w -= vi[4 * q + 3];
-        cr[q] = x;
-        ci[q] = y;
+        for (int q = 0; q < 4; ++q) {
+          float4& x = xr[c * 4 + q];
+          float4& y = xi[c * 4 + q];
+          x.x -= vr[4 * q]; x.y -= vr[4 * q + 1]; x.z -= vr[4 * q + 2]; x.w -= vr[4 * q + 3];
+          y.x -= vi[4 * q]; y.y -= vi[4 * q + 1]; y.z -= vi[4 * q + 2]; y.w -= vi[4 * q + 3];
+        }
       }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh.acc_empty[acc]);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        cr[q] = xr[q];
+        ci[q] = xi[q];
+      }
+      if (++acc == 2) { acc = 0; acc_phase ^= 1; }
     }
-  }
-  if (!ok || sh.failed) {
-    if (threadIdx.x == 0) atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(kTmemCols));
+                 "r"(kTmemColsP));
   }
 }
 
@@ -349,10 +417,8 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     return set_error(err, cap, AOSB_ERR_NULL, "tensor-core path needs a staging workspace");
   cudaStream_t st = (cudaStream_t)a->stream;
   const int np = a->n_pencils;
-  // The full 227 KB keeps every address a descriptor can form inside this
-  // CTA's shared memory.
-  const size_t smem = 232448;
-  static_assert(sizeof(TcShared) + 1024 <= 232448, "shared memory budget");
+  const size_t smem = sizeof(PShared) + 1024;
+  static_assert(sizeof(PShared) + 1024 <= 232448, "shared memory budget");
   static bool attr_done = false;
   if (!attr_done) {
     cudaError_t e = cudaFuncSetAttribute(schur_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -361,6 +427,9 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
       return set_error(err, cap, AOSB_ERR_CUDA, "schur_tc smem attribute: %s", cudaGetErrorString(e));
     attr_done = true;
   }
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   int64_t most = 0;
   for (int64_t k = 0; k < P->nb; ++k) {
     const int64_t items = (P->lb_off[k + 1] - P->lb_off[k]) + (P->ur_off[k + 1] - P->ur_off[k]);
@@ -377,10 +446,13 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     stage_kernel<<<dim3(nL + nU, np), 256, 0, st>>>(nL, nU, P->d_lb_slot + P->lb_off[k],
                                                    P->d_ur_slot + P->ur_off[k], P->n_slots,
                                                    a->factor, staging, pencil_stride);
-    const int64_t pairs = (int64_t)nL * nU;
-    schur_tc_kernel<<<dim3((unsigned)pairs, np), kTcThreads, smem, st>>>(
-        nU, nL, P->d_sc_slot + P->sc_off[k], P->n_slots, a->factor, staging, pencil_stride,
-        a->status);
+    const int64_t items = (int64_t)nL * nU * np;
+    if ((int64_t)nL * nU > INT32_MAX / 65536)
+      return set_error(err, cap, AOSB_ERR_SIZE, "too many Schur targets in one step");
+    const int grid = (int)(items < sms ? items : sms);
+    schur_tc_kernel<<<grid, kPThreads, smem, st>>>(nU, nL, nL * nU, np, P->d_sc_slot + P->sc_off[k],
+                                                   P->n_slots, a->factor, staging, pencil_stride,
+                                                   a->status);
     count_launches(2);
   }
   return launch_check(err, cap, "tensor-core factorization");

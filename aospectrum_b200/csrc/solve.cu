@@ -26,27 +26,33 @@ __device__ __forceinline__ size_t tile_base(int64_t p, int64_t n_slots, int64_t 
 
 enum DiagOp { kLinv = 0, kUinv = 1, kUinvH = 2, kLinvH = 3 };
 
-// Diagonal step: X_k <- op(D_kk) X_k over column strip blockIdx.x of width 32.
-// kLinv gathers rows through P_k first; kLinvH scatters rows through P_k^T.
+constexpr int kCopyBlocks = 4;  // CTAs that copy the diagonal result back
+
+// Diagonal step, out of place: Y = op(D_kk) X_k, one CTA per (32-column
+// strip, 32-row block, pencil).  kLinv gathers rows of X_k through P_k;
+// kLinvH stores row r of the product at row P_k[r] (x_k = P_k^T v_k).
+// Y is a per-pencil T x n_rhs scratch block; the update launch of the same
+// step copies it back into X_k.
 template <int T, int OP>
 __global__ void __launch_bounds__(kThreads) solve_diag_kernel(int k, int nrhs, int64_t n_pad,
                                                               const int32_t* __restrict__ diag_slot,
                                                               int64_t n_slots,
                                                               const float* __restrict__ factor,
                                                               const int32_t* __restrict__ pivots,
-                                                              float2* __restrict__ work) {
-  constexpr int BN = 32;
-  constexpr int TN = T == 32 ? 2 : 4;
-  constexpr int TM = (T / 4) * (BN / TN) == 256 ? 4 : ((T / 2) * (BN / TN) == 256 ? 2 : 1);
-  static_assert((T / TM) * (BN / TN) == 256, "layout");
-  __shared__ CgemmSmem<T, BN> sm;
-  const int p = blockIdx.y;
-  const int c0 = blockIdx.x * BN;
+                                                              const float2* __restrict__ work,
+                                                              float2* __restrict__ ytmp) {
+  constexpr int BM = 32, BN = 32, TM = 2, TN = 2;
+  static_assert((BM / TM) * (BN / TN) == 256, "layout");
+  __shared__ CgemmSmem<BM, BN> sm;
+  const int p = blockIdx.z;
+  const int c0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
   const float* D = factor + tile_base(p, n_slots, diag_slot[k], T);
   const int32_t* pv = pivots + (size_t)p * n_pad + (size_t)k * T;
-  float2* X = work + ((size_t)p * n_pad + (size_t)k * T) * nrhs;
+  const float2* X = work + ((size_t)p * n_pad + (size_t)k * T) * nrhs;
+  float2* Y = ytmp + (size_t)p * T * nrhs;
   float accr[TM][TN] = {}, acci[TM][TN] = {};
-  auto la = [&](int r, int q) -> float2 {
+  auto la = [&](int m, int q) -> float2 {
+    const int r = m0 + m;
     if (OP == kLinv) {
       if (q > r) return make_float2(0.f, 0.f);
       if (q == r) return make_float2(1.f, 0.f);
@@ -73,43 +79,51 @@ __global__ void __launch_bounds__(kThreads) solve_diag_kernel(int k, int nrhs, i
     const int row = OP == kLinv ? pv[q] : q;
     return X[(size_t)row * nrhs + col];
   };
-  cgemm_cta<T, BN, TM, TN>(accr, acci, T, sm, la, lb);
-  // Every CTA has read its whole column strip before this point.
+  cgemm_cta<BM, BN, TM, TN>(accr, acci, T, sm, la, lb);
 #pragma unroll
   for (int i = 0; i < TM; ++i)
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
-      const int r = cg_row<T, BN, TM, TN>(i), col = c0 + cg_col<T, BN, TM, TN>(j);
+      const int r = m0 + cg_row<BM, BN, TM, TN>(i), col = c0 + cg_col<BM, BN, TM, TN>(j);
       if (col >= nrhs) continue;
       const int row = OP == kLinvH ? pv[r] : r;
-      X[(size_t)row * nrhs + col] = make_float2(accr[i][j], acci[i][j]);
+      Y[(size_t)row * nrhs + col] = make_float2(accr[i][j], acci[i][j]);
     }
 }
 
 enum UpdOp { kPlain = 0, kConjT = 1 };
 
-// Update step: X_i -= op(F_t) X_k for the listed tiles.  blockIdx.x =
-// (item, row half, column strip); op = plain tile or conjugate transpose.
+// Update step: X_i -= op(F_t) Y for the listed tiles, Y = the step's
+// diagonal result.  blockIdx.x = (item, row block, column strip); the last
+// `copy_blocks` CTAs copy Y into X_k.  op = plain tile or conjugate transpose.
 template <int T, int OP>
 __global__ void __launch_bounds__(kThreads) solve_update_kernel(
     int k, int n_items, int nrhs, int64_t n_pad, const int32_t* __restrict__ tiles,
     const int32_t* __restrict__ slots, int64_t n_slots, const float* __restrict__ factor,
-    float2* __restrict__ work) {
+    float2* __restrict__ work, const float2* __restrict__ ytmp) {
   constexpr int BM = T >= 64 ? 64 : 32;
   constexpr int BN = 32;
-  constexpr int TM = BM == 64 ? 4 : 2, TN = BM == 64 ? 2 : 2;
+  constexpr int TM = BM == 64 ? 4 : 2, TN = 2;
   static_assert((BM / TM) * (BN / TN) == 256, "layout");
   constexpr int kRowBlocks = T / BM;
   __shared__ CgemmSmem<BM, BN> sm;
   const int p = blockIdx.y;
   const int ncs = (nrhs + BN - 1) / BN;
+  const int work_blocks = n_items * kRowBlocks * ncs;
+  const float2* Y = ytmp + (size_t)p * T * nrhs;
+  if ((int)blockIdx.x >= work_blocks) {
+    // copy-back CTAs
+    const int cb = blockIdx.x - work_blocks;
+    float2* Xk = work + ((size_t)p * n_pad + (size_t)k * T) * nrhs;
+    const int total = T * nrhs;
+    for (int e = cb * kThreads + threadIdx.x; e < total; e += kCopyBlocks * kThreads) Xk[e] = Y[e];
+    return;
+  }
   const int item = blockIdx.x / (kRowBlocks * ncs);
   const int rem = blockIdx.x % (kRowBlocks * ncs);
   const int m0 = (rem / ncs) * BM, c0 = (rem % ncs) * BN;
-  if (item >= n_items) return;
   const int i = tiles[item];
   const float* F = factor + tile_base(p, n_slots, slots[item], T);
-  const float2* Xk = work + ((size_t)p * n_pad + (size_t)k * T) * nrhs;
   float2* Xi = work + ((size_t)p * n_pad + (size_t)i * T) * nrhs;
   float accr[TM][TN] = {}, acci[TM][TN] = {};
   auto la = [&](int m, int q) -> float2 {
@@ -124,7 +138,7 @@ __global__ void __launch_bounds__(kThreads) solve_update_kernel(
   auto lb = [&](int q, int c) -> float2 {
     const int col = c0 + c;
     if (col >= nrhs) return make_float2(0.f, 0.f);
-    return Xk[(size_t)q * nrhs + col];
+    return Y[(size_t)q * nrhs + col];
   };
   cgemm_cta<BM, BN, TM, TN>(accr, acci, T, sm, la, lb);
 #pragma unroll
@@ -148,26 +162,26 @@ int run_solve(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t
   constexpr int BM = T >= 64 ? 64 : 32;
   const int rowblocks = T / BM;
   float2* W = (float2*)a->work;
+  float2* Y = (float2*)a->scratch;
   auto diag = [&](int k, int op) {
     count_launches(1);
-    dim3 g(ncs, np);
+    dim3 g(ncs, T / 32, np);
     switch (op) {
-      case kLinv: solve_diag_kernel<T, kLinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W); break;
-      case kUinv: solve_diag_kernel<T, kUinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W); break;
-      case kUinvH: solve_diag_kernel<T, kUinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W); break;
-      default: solve_diag_kernel<T, kLinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W); break;
+      case kLinv: solve_diag_kernel<T, kLinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y); break;
+      case kUinv: solve_diag_kernel<T, kUinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y); break;
+      case kUinvH: solve_diag_kernel<T, kUinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y); break;
+      default: solve_diag_kernel<T, kLinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y); break;
     }
   };
   auto update = [&](int k, const std::vector<int32_t>& off, const int32_t* dtiles,
                     const int32_t* dslots, int op) {
     const int n = off[k + 1] - off[k];
-    if (n == 0) return;
-    dim3 g((unsigned)(n * rowblocks * ncs), np);
+    dim3 g((unsigned)(n * rowblocks * ncs + kCopyBlocks), np);
     count_launches(1);
     if (op == kPlain)
-      solve_update_kernel<T, kPlain><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + off[k], dslots + off[k], P->n_slots, a->factor, W);
+      solve_update_kernel<T, kPlain><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + off[k], dslots + off[k], P->n_slots, a->factor, W, Y);
     else
-      solve_update_kernel<T, kConjT><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + off[k], dslots + off[k], P->n_slots, a->factor, W);
+      solve_update_kernel<T, kConjT><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + off[k], dslots + off[k], P->n_slots, a->factor, W, Y);
   };
   const int nb = (int)P->nb;
   if (!a->adjoint) {
@@ -276,6 +290,11 @@ __global__ void shifted_residual_kernel(int64_t n, int nrhs, const int64_t* __re
 
 extern "C" {
 
+size_t aosb_solve_scratch_bytes(const aosb_plan_t* P, int32_t np, int32_t nrhs) {
+  if (P == nullptr || np <= 0 || nrhs <= 0) return 0;
+  return (size_t)np * (size_t)P->T * (size_t)nrhs * sizeof(float2);
+}
+
 int aosb_solve(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* err, size_t cap) {
   using aosb::set_error;
   if (P == nullptr || a == nullptr) return set_error(err, cap, AOSB_ERR_NULL, "null argument");
@@ -283,7 +302,7 @@ int aosb_solve(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* err, siz
     return set_error(err, cap, AOSB_ERR_ABI, "solve args ABI mismatch");
   if (a->n_pencils <= 0 || a->n_pencils > 65535 || a->n_rhs <= 0 || a->n_rhs > 256)
     return set_error(err, cap, AOSB_ERR_BATCH, "invalid pencil or right-hand-side count");
-  if (a->factor == nullptr || a->pivots == nullptr || a->work == nullptr)
+  if (a->factor == nullptr || a->pivots == nullptr || a->work == nullptr || a->scratch == nullptr)
     return set_error(err, cap, AOSB_ERR_NULL, "required pointer is null");
   if (!P->uploaded) return set_error(err, cap, AOSB_ERR_ARGUMENT, "call aosb_plan_upload first");
   switch (P->T) {

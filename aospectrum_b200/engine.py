@@ -271,6 +271,7 @@ class BandEngine:
         q = probe_block(self.n, self.settings)
         self.probes = torch.from_numpy(q.astype(np.complex128)).to(self.device)
         self._gram_scratch = None
+        self._solve_scratch = None
         self.last_stats: dict[str, Any] = {}
         # optional device timing of every factorization call (CUDA events)
         self.profile_factor = False
@@ -318,6 +319,7 @@ class BandEngine:
         per = lib.aosb_factor_bytes(self.plan.handle, 1) + 4 * info.n_pad + 4
         per += 8 * info.n_pad * n_rhs * 2          # normal + adjoint solve blocks (complex64)
         per += 16 * self.n * n_rhs * 3             # x, r and adjoint x (complex128)
+        per += lib.aosb_factor_workspace_bytes(self.plan.handle, 1, native.PRECISION_BF16X3)
         return int(per)
 
     def max_pencils(self, n_rhs: int) -> int:
@@ -487,8 +489,12 @@ class BandEngine:
         # gather the rhs of each pencil's k into the pencil-major residual buffer
         kidx = torch.tensor([w.k for w in batch], dtype=torch.long, device=self.device)
         b = rhs.index_select(0, kidx).contiguous()
+        need = native.library().aosb_solve_scratch_bytes(self.plan.handle, np_, L)
+        if self._solve_scratch is None or self._solve_scratch.numel() < need:
+            self._solve_scratch = torch.empty(max(need, 16), dtype=torch.uint8, device=self.device)
         sa = native.SolveArgs(native.ABI_VERSION, native.C.sizeof(native.SolveArgs), np_, L,
-                              adjoint, 0, factor.data_ptr(), pivots.data_ptr(), wn.data_ptr(), st)
+                              adjoint, 0, factor.data_ptr(), pivots.data_ptr(), wn.data_ptr(),
+                              self._solve_scratch.data_ptr(), st)
         for it in range(steps + 1):
             src = b if it == 0 else rr
             native.call("aosb_gather_rhs", self.plan.handle, np_, L, src.data_ptr(), n * L,

@@ -55,6 +55,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--accuracy-kpoints", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--max-pencils", type=int, default=0,
+                    help="cap on pencils factored together (0 = by memory)")
     return ap.parse_args()
 
 
@@ -215,7 +217,8 @@ def main() -> None:
                             moment_size=w.moment_size)
     eng = BandEngine(bundle, settings,
                      EngineSettings(precision=args.precision,
-                                    tensor_cores=bool(args.tensor_cores)), device=dev)
+                                    tensor_cores=bool(args.tensor_cores),
+                                    max_pencils=args.max_pencils), device=dev)
     kpts = kp.fractional_points
     nk_step = args.kpoints_per_step or (1 if w.spec.n_orbitals > 4000 else 8)
 

@@ -265,6 +265,7 @@ int aosb_factor(const aosb_plan_t *plan, const aosb_factor_args_v1 *args,
  * adjoint = 0 solves A X = B, adjoint = 1 solves A^H X = B (the conjugate
  * shift of a contour node pair reuses one factorization this way).
  * work: device [n_pencils][n_pad][n_rhs] complex64, overwritten.
+ * scratch: device, aosb_solve_scratch_bytes(plan, n_pencils, n_rhs).
  * ------------------------------------------------------------------------ */
 typedef struct {
   uint32_t abi_version;
@@ -276,9 +277,11 @@ typedef struct {
   const float *factor;
   const int32_t *pivots;
   aosb_complex64 *work;
+  void *scratch;
   void *stream;
 } aosb_solve_args_v1;
 
+size_t aosb_solve_scratch_bytes(const aosb_plan_t *plan, int32_t n_pencils, int32_t n_rhs);
 int aosb_solve(const aosb_plan_t *plan, const aosb_solve_args_v1 *args,
                char *err, size_t err_cap);
 

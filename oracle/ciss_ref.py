@@ -36,6 +36,9 @@ class RefCissResult:
 
 def contour(lower: float, upper: float, n_points: int = 32, scale: float = 0.1,
             guard: float = 1.0e-5):
+    # Python floats, as the reference's EnergyInterval stores them (numpy
+    # float64 scalars would change the float32/complex64 promotion below).
+    lower, upper = float(lower), float(upper)
     lo = lower - 2.0 * guard
     hi = upper + 2.0 * guard
     centre = 0.5 * (lo + hi)

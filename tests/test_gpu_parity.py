@@ -116,8 +116,10 @@ def _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=0, adjoint=0, s
     x = torch.zeros((P, n, L), dtype=torch.complex128, device=dv)
     r = torch.zeros_like(x)
     w = torch.empty((P, info.n_pad, L), dtype=torch.complex64, device=dv)
+    scratch = torch.empty(max(16, lib.aosb_solve_scratch_bytes(plan.handle, P, L)),
+                          dtype=torch.uint8, device=dv)
     sa = native.SolveArgs(native.ABI_VERSION, native.C.sizeof(native.SolveArgs), P, L, adjoint, 0,
-                          factor.data_ptr(), piv.data_ptr(), w.data_ptr(), st)
+                          factor.data_ptr(), piv.data_ptr(), w.data_ptr(), scratch.data_ptr(), st)
     zz = torch.conj_physical(z) if adjoint else z
     for it in range(steps + 1):
         src = b if it == 0 else r

@@ -1,0 +1,174 @@
+"""The C-ABI library without a GPU: it loads, exports every symbol the
+header declares, and its host-only entry points (pattern build, symbolic
+analysis, request validation) behave."""
+
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import bundles
+from aospectrum_b200 import native
+from oracle import bloch_ref
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "aospectrum_b200.h"
+
+
+def header_functions():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(aos\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = native.library()
+    names = header_functions()
+    assert len(names) >= 25
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in native.exported_symbols(), name
+    assert lib.aosb_abi_version() == native.ABI_VERSION
+    assert b"sm_100a" in lib.aosb_build_info()
+
+
+def _bloch_create(b, drop_block=None):
+    ops = b.operators
+    keep = np.ones(ops.n_blocks, bool)
+    if drop_block is not None:
+        keep[drop_block] = False
+    rows = np.ascontiguousarray(ops.row_atom[keep], np.int32)
+    cols = np.ascontiguousarray(ops.col_atom[keep], np.int32)
+    sh = np.ascontiguousarray(ops.lattice_shift[keep], np.int32)
+    sizes = np.diff(ops.block_offsets)[keep]
+    bo = np.concatenate(([0], np.cumsum(sizes))).astype(np.int64)
+    off = np.ascontiguousarray(b.basis.atom_offsets, np.int64)
+    h = C.c_void_p()
+    buf = C.create_string_buffer(512)
+    rc = native.library().aosb_bloch_create(b.n_orbitals, b.basis.n_atoms, off.ctypes.data,
+                                            int(keep.sum()), rows.ctypes.data, cols.ctypes.data,
+                                            sh.ctypes.data, bo.ctypes.data, C.byref(h), buf, 512)
+    return rc, h, buf.value
+
+
+@pytest.mark.parametrize("name", ["tiny2d", "tiny3d", "small2d"])
+def test_host_pattern_builder_matches_reference(name, golden):
+    b = getattr(bundles, name)()
+    rc, h, _ = _bloch_create(b)
+    assert rc == 0
+    lib = native.library()
+    nnz, nsh = C.c_int64(), C.c_int64()
+    lib.aosb_bloch_info(h, C.byref(nnz), C.byref(nsh))
+    ip = np.empty(b.n_orbitals + 1, np.int64)
+    ix = np.empty(nnz.value, np.int32)
+    shifts = np.empty((nsh.value, 3), np.int32)
+    bsh = np.empty(b.operators.n_blocks, np.int32)
+    lib.aosb_bloch_export(h, ip.ctypes.data, ix.ctypes.data, shifts.ctypes.data, bsh.ctypes.data)
+    pat = bloch_ref.build_pattern(b)
+    assert np.array_equal(ip, pat.indptr) and np.array_equal(ix, pat.indices)
+    assert np.array_equal(shifts, pat.shifts)
+    lib.aosb_bloch_destroy(h)
+
+
+def test_host_pattern_builder_rejects_non_hermitian_topology():
+    b = bundles.tiny2d()
+    # drop one off-diagonal block: its mirror loses its partner
+    off_diag = int(np.flatnonzero(b.operators.row_atom != b.operators.col_atom)[0])
+    rc, h, msg = _bloch_create(b, drop_block=off_diag)
+    assert rc == 41 and b"not Hermitian" in msg
+
+
+def _plan(ip, ix, n, tile=32, ordering=1, sv=None):
+    opts = native.PlanOptions(native.ABI_VERSION, C.sizeof(native.PlanOptions), tile, ordering,
+                              4 * tile, 1)
+    h = C.c_void_p()
+    buf = C.create_string_buffer(512)
+    ip = np.ascontiguousarray(ip, np.int64)
+    ix = np.ascontiguousarray(ix, np.int32)
+    rc = native.library().aosb_plan_create(n, ip.ctypes.data, ix.ctypes.data,
+                                           None if sv is None else sv.ctypes.data,
+                                           0 if sv is None else sv.size - 1, C.byref(opts),
+                                           C.byref(h), buf, 512)
+    return rc, h, buf.value
+
+
+@pytest.mark.parametrize("name,tile,ordering", [("tiny3d", 32, 1), ("tiny3d", 32, 0),
+                                                ("small2d", 64, 1), ("c1", 128, 1),
+                                                ("c1", 64, 0)])
+def test_symbolic_plan_is_a_closed_fill_pattern(name, tile, ordering):
+    b = getattr(bundles, name)()
+    pat = bloch_ref.build_pattern(b)
+    n = b.n_orbitals
+    rc, h, msg = _plan(pat.indptr, pat.indices, n, tile, ordering,
+                       np.ascontiguousarray(b.basis.atom_offsets, np.int64))
+    assert rc == 0, msg
+    lib = native.library()
+    info = native.PlanInfo()
+    lib.aosb_plan_info(h, C.byref(info))
+    perm = np.empty(info.n_pad, np.int32)
+    lib.aosb_plan_export_perm(h, perm.ctypes.data)
+    assert sorted(perm[perm >= 0].tolist()) == list(range(n))
+    assert info.n_pad % tile == 0 and info.n_tiles * tile == info.n_pad
+    nb = info.n_tiles
+    slot = np.empty(nb * nb, np.int32)
+    lib.aosb_plan_export_slots(h, slot.ctypes.data)
+    nz = slot.reshape(nb, nb) >= 0
+    assert int(nz.sum()) == info.n_slots
+    # A's tile pattern is covered
+    pinv = np.empty(n, np.int64)
+    pinv[perm[perm >= 0]] = np.flatnonzero(perm >= 0)
+    rows = np.repeat(np.arange(n), np.diff(pat.indptr))
+    assert nz[pinv[rows] // tile, pinv[pat.indices] // tile].all()
+    # closed under elimination: L(i,k) and U(k,j) nonzero => (i,j) nonzero
+    for k in range(nb):
+        below = np.flatnonzero(nz[k + 1:, k]) + k + 1
+        right = np.flatnonzero(nz[k, k + 1:]) + k + 1
+        assert nz[np.ix_(below, right)].all()
+    assert info.factor_flops >= info.factor_flops_alg > 0
+    lib.aosb_plan_destroy(h)
+
+
+def test_symbolic_plan_rejects_bad_patterns():
+    ip = np.array([0, 2, 3], np.int64)
+    assert _plan(ip, np.array([0, 1, 0], np.int32), 2)[0] == 33      # row 1 misses its diagonal
+    assert _plan(ip, np.array([1, 0, 1], np.int32), 2)[0] == 32      # unsorted columns
+    assert _plan(ip, np.array([0, 5, 1], np.int32), 2)[0] == 31      # column out of range
+    assert _plan(np.array([0, 1, 2], np.int64), np.array([0, 1], np.int32), 2, tile=48)[0] == 53
+    bad = native.PlanOptions(99, C.sizeof(native.PlanOptions), 32, 1, 128, 1)
+    h = C.c_void_p()
+    rc = native.library().aosb_plan_create(2, np.array([0, 1, 2], np.int64).ctypes.data,
+                                           np.array([0, 1], np.int32).ctypes.data, None, 0,
+                                           C.byref(bad), C.byref(h), None, 0)
+    assert rc == 10
+
+
+def _ubatch(n=3, batch=1, rhs=1, values=None, indptr=None, indices=None, abi=None):
+    indptr = np.array([0, 1, 2, 3], np.int32) if indptr is None else indptr
+    indices = np.array([0, 1, 2], np.int32) if indices is None else indices
+    nnz = int(indices.size)
+    values = np.ones(batch * nnz, np.complex64) if values is None else values
+    r = np.ones(batch * n * rhs, np.complex64)
+    sol = np.zeros_like(r)
+    req = native.UbatchRequest(abi or native.ABI_VERSION, C.sizeof(native.UbatchRequest), n, nnz,
+                               batch, rhs, indptr.ctypes.data, indices.ctypes.data,
+                               values.ctypes.data, r.ctypes.data, sol.ctypes.data)
+    res = native.UbatchResult()
+    rc = native.library().aospectrum_b200_solve_complex64_ubatch_v1(C.byref(req), C.byref(res))
+    return rc, res
+
+
+def test_ubatch_request_validation_codes():
+    """The reference's validation codes (native/src/aospectrum_cudss_complex64_
+    ubatch.c:136-241), all raised before any device call."""
+    assert _ubatch(abi=7)[1].status == 10
+    assert _ubatch(batch=65)[1].status == 12
+    assert _ubatch(rhs=257)[1].status == 12
+    assert _ubatch(indptr=np.array([0, 1, 2, 2], np.int32))[1].status == 14
+    assert _ubatch(indices=np.array([0, 1, 1], np.int32),
+                   indptr=np.array([0, 1, 2, 3], np.int32))[1].status == 33
+    vals = np.ones(3, np.complex64)
+    vals[1] = np.inf
+    rc, res = _ubatch(values=vals)
+    assert rc != 0 and res.status == 35 and b"non-finite" in res.error_message
