@@ -214,6 +214,26 @@ class SymbolicPlan:
             self.handle = None
 
 
+class CsrPattern:
+    """A user CSR pattern on the device (for CISS on given H, S matrices)."""
+
+    def __init__(self, n: int, indptr: np.ndarray, indices: np.ndarray, device: Any) -> None:
+        torch = _torch()
+        self.n = int(n)
+        self.indptr = np.ascontiguousarray(indptr, dtype=np.int64)
+        self.indices = np.ascontiguousarray(indices, dtype=np.int32)
+        if self.indptr.shape != (self.n + 1,) or self.indptr[0] != 0 or \
+                self.indptr[-1] != self.indices.size:
+            raise InputError("CSR indptr endpoints are invalid")
+        self.nnz = int(self.indices.size)
+        self._ip = torch.from_numpy(self.indptr).to(device)
+        self._ix = torch.from_numpy(self.indices).to(device)
+        self.d_indptr, self.d_indices = self._ip.data_ptr(), self._ix.data_ptr()
+
+    def close(self) -> None:
+        self._ip = self._ix = None
+
+
 @dataclass
 class PencilWork:
     """One factorization: k row, shift, and the nodes it serves."""
@@ -247,26 +267,38 @@ def pencil_schedule(n_k: int, shifts: np.ndarray, pair: bool) -> list[PencilWork
 class BandEngine:
     """Device-resident Band solver for one bundle."""
 
-    def __init__(self, bundle: LocalizedOperatorBundle, settings: CissSettings | None = None,
-                 engine: EngineSettings | None = None, device: Any = None) -> None:
+    def __init__(self, bundle: LocalizedOperatorBundle | None,
+                 settings: CissSettings | None = None, engine: EngineSettings | None = None,
+                 device: Any = None, *, csr: tuple[int, np.ndarray, np.ndarray] | None = None
+                 ) -> None:
         torch = _torch()
         self.bundle = bundle
         self.settings = settings or CissSettings()
         self.engine = engine or EngineSettings()
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None
                                    else torch.device(device).index or 0)
-        self.n = bundle.n_orbitals
+        t0 = perf_counter()
+        if bundle is not None:
+            self.n = bundle.n_orbitals
+            self.bloch = BlochDevice(bundle, self.device)
+            self.pattern = self.bloch
+            supervariables = np.asarray(bundle.basis.atom_offsets)
+        else:
+            if csr is None:
+                raise InputError("BandEngine needs a bundle or a CSR pattern")
+            self.n = int(csr[0])
+            self.bloch = None
+            self.pattern = CsrPattern(csr[0], csr[1], csr[2], self.device)
+            supervariables = None
         if self.settings.search_dimension >= self.n:
             raise SolverError("CISS search dimension must be smaller than matrix dimension")
-        t0 = perf_counter()
-        self.bloch = BlochDevice(bundle, self.device)
         self.pattern_seconds = perf_counter() - t0
         t0 = perf_counter()
         use_tc = self.engine.precision == "mixed" and self.engine.tensor_cores
         tile = self.engine.tile or (128 if use_tc else choose_tile(self.n))
-        self.plan = SymbolicPlan(self.n, self.bloch.indptr, self.bloch.indices, tile=tile,
-                                 supervariables=np.asarray(bundle.basis.atom_offsets),
-                                 ordering=self.engine.ordering, device=self.device)
+        self.plan = SymbolicPlan(self.n, self.pattern.indptr, self.pattern.indices, tile=tile,
+                                 supervariables=supervariables, ordering=self.engine.ordering,
+                                 device=self.device)
         self.analysis_seconds = perf_counter() - t0
         q = probe_block(self.n, self.settings)
         self.probes = torch.from_numpy(q.astype(np.complex128)).to(self.device)
@@ -286,7 +318,7 @@ class BandEngine:
     def _spmm(self, values, x, y) -> None:
         """y = A x for one k (values [nnz] complex64)."""
         n, m = x.shape
-        native.call("aosb_spmm", n, m, self.bloch.d_indptr, self.bloch.d_indices,
+        native.call("aosb_spmm", n, m, self.pattern.d_indptr, self.pattern.d_indices,
                     values.data_ptr(), x.data_ptr(), x.stride(0), y.data_ptr(), y.stride(0),
                     self._stream())
 
@@ -360,6 +392,20 @@ class BandEngine:
         return SparsePair(sparse.csr_matrix((hv, ix, ip), shape=shape, copy=False),
                           sparse.csr_matrix((sv, ix, ip), shape=shape, copy=False), kp)
 
+    def solve_values(self, h_values, s_values, interval: EnergyInterval) -> list[CissResult]:
+        """CISS on given H, S value rows (complex64, [n_k, nnz] or [nnz]) of
+        this engine's pattern; host arrays are uploaded."""
+        torch = _torch()
+        h = torch.as_tensor(np.asarray(h_values, dtype=np.complex64)).to(self.device)
+        s = torch.as_tensor(np.asarray(s_values, dtype=np.complex64)).to(self.device)
+        h = h.reshape(-1, self.pattern.nnz).contiguous()
+        s = s.reshape(-1, self.pattern.nnz).contiguous()
+        if h.shape != s.shape:
+            raise InputError("H and S values differ in shape")
+        with torch.cuda.device(self.device):
+            torch.cuda.reset_peak_memory_stats(self.device)
+            return self._ciss(h, s, interval, {}, perf_counter())
+
     def solve_kpoints(self, kpoints: Sequence[Sequence[float]], interval: EnergyInterval):
         """CISS for several k points; returns (results, assembly_seconds)."""
         torch = _torch()
@@ -373,12 +419,24 @@ class BandEngine:
 
     def _solve(self, kp: np.ndarray, interval: EnergyInterval):
         torch = _torch()
+        dev = self.device
+        torch.cuda.reset_peak_memory_stats(dev)
+        t0 = perf_counter()
+        hvals, svals = self.bloch.apply(kp)
+        torch.cuda.synchronize(dev)
+        assembly = perf_counter() - t0
+        results = self._ciss(hvals, svals, interval, {"bloch_assembly": assembly}, t0)
+        return results, [assembly / kp.shape[0]] * kp.shape[0]
+
+    def _ciss(self, hvals, svals, interval: EnergyInterval, stages: dict[str, float],
+              total0: float) -> list[CissResult]:
+        """CISS for the n_k value rows of (hvals, svals) on self.pattern."""
+        torch = _torch()
         st = self.settings
         mixed = self.engine.precision == "mixed"
         n, L, M = self.n, st.block_size, st.moment_size
-        nk = kp.shape[0]
+        nk = hvals.shape[0]
         dev = self.device
-        stages: dict[str, float] = {}
 
         def tick(name: str, t0: float) -> float:
             torch.cuda.synchronize(dev)
@@ -386,11 +444,7 @@ class BandEngine:
             stages[name] = stages.get(name, 0.0) + (t1 - t0)
             return t1
 
-        total0 = t = perf_counter()
-        torch.cuda.reset_peak_memory_stats(dev)
-        hvals, svals = self.bloch.apply(kp)
-        t = tick("bloch_assembly", t)
-        assembly = stages["bloch_assembly"] / nk
+        t = perf_counter()
         shifts, nodes, weights = contour_geometry(interval, st)
         coef = moment_coefficients(shifts, nodes, weights, M)
         rhs = torch.empty((nk, n, L), dtype=torch.complex128, device=dev)
@@ -469,14 +523,12 @@ class BandEngine:
             results.append(self._subspace(hvals[k], svals[k], mom[k], interval, stages, nk))
         peak = int(torch.cuda.max_memory_allocated(dev))
         total = perf_counter() - total0
-        out = []
         for res in results:
             res.stage_seconds["solver_total"] = total / nk
             res.peak_gpu_memory_bytes = peak
-            out.append(res)
         self.last_stats = {"factorizations": n_factor, "pencil_batch": cap,
                            "stage_seconds": dict(stages)}
-        return out, [assembly] * nk
+        return results
 
     def _solve_refined(self, batch, pk, z, hvals, svals, rhs, factor, pivots, wn, xn, rr,
                        adjoint: int, steps: int) -> None:
@@ -503,9 +555,9 @@ class BandEngine:
             native.call("aosb_scatter_solution", self.plan.handle, np_, L, wn.data_ptr(),
                         xn.data_ptr(), 1 if it > 0 else 0, st)
             if it < steps:
-                native.call("aosb_shifted_residual", n, L, np_, self.bloch.d_indptr,
-                            self.bloch.d_indices, hvals.data_ptr(), svals.data_ptr(),
-                            self.bloch.nnz, pk.data_ptr(), z.contiguous().data_ptr(),
+                native.call("aosb_shifted_residual", n, L, np_, self.pattern.d_indptr,
+                            self.pattern.d_indices, hvals.data_ptr(), svals.data_ptr(),
+                            self.pattern.nnz, pk.data_ptr(), z.contiguous().data_ptr(),
                             b.data_ptr(), n * L, xn.data_ptr(), rr.data_ptr(), st)
 
     def _subspace(self, h, s, mom, interval: EnergyInterval, stages: dict[str, float],
@@ -556,5 +608,5 @@ class BandEngine:
                           not saturated)
 
     def close(self) -> None:
-        self.bloch.close()
+        self.pattern.close()
         self.plan.close()

@@ -55,6 +55,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--accuracy-kpoints", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--refinement-steps", type=int, default=-1,
+                    help="FP64 refinement sweeps per mixed solve (-1 = engine default)")
     ap.add_argument("--max-pencils", type=int, default=0,
                     help="cap on pencils factored together (0 = by memory)")
     return ap.parse_args()
@@ -218,7 +220,9 @@ def main() -> None:
     eng = BandEngine(bundle, settings,
                      EngineSettings(precision=args.precision,
                                     tensor_cores=bool(args.tensor_cores),
-                                    max_pencils=args.max_pencils), device=dev)
+                                    max_pencils=args.max_pencils,
+                                    **({"refinement_steps": args.refinement_steps}
+                                       if args.refinement_steps >= 0 else {})), device=dev)
     kpts = kp.fractional_points
     nk_step = args.kpoints_per_step or (1 if w.spec.n_orbitals > 4000 else 8)
 
@@ -297,6 +301,8 @@ def main() -> None:
                    "block_size": w.block_size, "moment_size": w.moment_size,
                    "window_ev": list(w.window_ev), "precision": args.precision,
                    "tile": info.tile, "ordering": eng.plan.ordering,
+                   "refinement_steps": eng.engine.refinement_steps if args.precision == "mixed"
+                   else 0,
                    "factorizations_per_step": stats.get("factorizations"),
                    "pencil_batch": stats.get("pencil_batch"),
                    "l2": "inputs larger than L2 (factor storage %.2f GB per pencil)" % (

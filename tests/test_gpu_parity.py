@@ -294,3 +294,45 @@ def test_engine_ciss_matches_reference(key, precision, tc, golden, torch):
         assert res[0].maximum_residual_ev <= max(case["max_residual_ev"], 1e-6) * 1.01
     finally:
         eng.close()
+
+
+def test_dropin_solver_classes(golden, torch):
+    """B200CissSolver / NativeB200ShiftSolver behave like the reference's
+    CudssCissSolver / NativeCudssShiftSolver on host CSR matrices."""
+    from aospectrum_b200.ciss import CissSettings
+    from aospectrum_b200.data import EnergyInterval
+    from aospectrum_b200.solvers import B200CissSolver, NativeB200ShiftSolver
+    from fake_engine import OracleEngine
+
+    case = json.loads((golden / "manifest.json").read_text())["ciss"]["small2d_k2"]
+    ref_e = np.sort(np.load(golden / "ciss.npz")["small2d_k2_energies"])
+    b = bundles.small2d()
+    settings = CissSettings(integration_points=case["integration_points"],
+                            block_size=case["block_size"], moment_size=case["moment_size"])
+    pair = OracleEngine(b, settings, None).host_pair(bundles.KPOINTS[case["k_index"]])
+    solver = B200CissSolver(settings)
+    try:
+        res = solver.solve_interval(pair, EnergyInterval(*case["interval"]))
+        got = np.sort(res.energies_ev.astype(np.float64))
+        assert got.size == ref_e.size and np.max(np.abs(got - ref_e)) < EIG_TOL_EV
+        assert res.complete
+    finally:
+        solver.close()
+    shifted = NativeB200ShiftSolver()
+    try:
+        rng = np.random.default_rng(5)
+        rhs = (rng.standard_normal((b.n_orbitals, 6)) + 1j * rng.standard_normal(
+            (b.n_orbitals, 6))).astype(np.complex64)
+        shifts = np.asarray([-2.3 + 0.01j, -2.0 + 0.1j], dtype=np.complex64)
+        out = shifted.solve_shifted(pair, shifts, rhs)
+        assert out.solutions.shape == (2, b.n_orbitals, 6)
+        from scipy.sparse import linalg as spl
+
+        for i, z in enumerate(shifts):
+            a = (pair.hamiltonian.astype(np.complex128)
+                 - complex(z) * pair.overlap.astype(np.complex128)).tocsc()
+            ref = spl.splu(a).solve(rhs.astype(np.complex128))
+            assert np.linalg.norm(out.solutions[i] - ref) / np.linalg.norm(ref) < 1e-6
+        assert "numeric_factorization" in out.stage_seconds
+    finally:
+        shifted.close()

@@ -172,3 +172,20 @@ def test_ubatch_request_validation_codes():
     vals[1] = np.inf
     rc, res = _ubatch(values=vals)
     assert rc != 0 and res.status == 35 and b"non-finite" in res.error_message
+
+
+def test_shift_session_argument_checks():
+    from aospectrum_b200.solvers import B200ShiftSession
+
+    with pytest.raises(ValueError):
+        B200ShiftSession([0, 1], [0], 2)
+    with pytest.raises(ValueError):
+        B200ShiftSession([0, 1, 2], [0, 1], 2, "float32")
+    s = B200ShiftSession([0, 1, 2], [0, 1], 2)
+    with pytest.raises(ValueError, match="1 through 64"):
+        s.solve(np.ones(2), np.ones(2), np.zeros(65), np.ones((2, 1)))
+    with pytest.raises(ValueError, match="RHS"):
+        s.solve(np.ones(2), np.ones(2), np.zeros(1), np.ones((3, 1)))
+    s.close()
+    with pytest.raises(RuntimeError, match="closed"):
+        s.solve(np.ones(2), np.ones(2), np.zeros(1), np.ones((2, 1)))
