@@ -7,6 +7,8 @@
 // problems and the reported residuals carry FP64 accuracy.
 #include "common.cuh"
 
+#include <mutex>
+
 namespace aosb {
 namespace {
 
@@ -279,4 +281,73 @@ int aosb_column_norms(int64_t n, int32_t m, const aosb_complex128* a, const aosb
   return aosb::launch_check(err, cap, "column_norms");
 }
 
-}  // extern "C"
+// ---------------------------------------------------------------------------
+// Gram product without any allocation, for callers that cannot allocate
+// device memory at the point of the call: code running inside another
+// framework's stream-ordered memory pool or under a memory cap that forbids
+// new cudaMalloc, real-time or callback contexts where an allocation could
+// block or deadlock, and embedders that must not grow the device heap after
+// start-up.  The partial sums live in one file-scope device array of
+// kNoAllocGramBytes (16 MiB); every GPU that loads this library's device
+// code holds it until the process exits.
+constexpr size_t kNoAllocGramBytes = (size_t)16 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_gram_scratch[kNoAllocGramBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+}  // namespace
+
+}  // namespace aosb
+
+extern "C" int aosb_gram_noalloc(int64_t n, int32_t p, int32_t q, const aosb_complex128* x,
+                                 int64_t ldx, const aosb_complex128* y, int64_t ldy,
+                                 aosb_complex128* g, void* stream, char* err, size_t cap) {
+  using namespace aosb;
+  if (x == nullptr || y == nullptr || g == nullptr)
+    return set_error(err, cap, AOSB_ERR_NULL, "null argument");
+  if (n <= 0 || p <= 0 || q <= 0 || ldx < p || ldy < q)
+    return set_error(err, cap, AOSB_ERR_ARGUMENT, "invalid gram shape");
+  const size_t need = aosb_gram_scratch_bytes(n, p, q);
+  if (need > kNoAllocGramBytes)
+    return set_error(err, cap, AOSB_ERR_SIZE,
+                     "aosb_gram_noalloc: n=%lld, p=%d, q=%d needs %zu bytes of partial sums, "
+                     "more than its fixed %zu-byte scratch (ceil(n/512)*p*q*16 must not exceed "
+                     "it); use aosb_gram with caller-provided scratch",
+                     (long long)n, p, q, need, kNoAllocGramBytes);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess)
+    return set_error(err, cap, AOSB_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices)
+    return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "device index %d not supported", dev);
+  void* scratch = nullptr;
+  {
+    // First call on a device: resolve the array's device address once, with
+    // that device current (a synchronous runtime call; make this first call
+    // before any stream capture).
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (g_noalloc_ptr[dev] == nullptr) {
+      void* ptr = nullptr;
+      e = cudaGetSymbolAddress(&ptr, g_noalloc_gram_scratch);
+      if (e != cudaSuccess || ptr == nullptr)
+        return set_error(err, cap, AOSB_ERR_CUDA, "cudaGetSymbolAddress failed: %s",
+                         cudaGetErrorString(e));
+      g_noalloc_ptr[dev] = ptr;
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  // Nothing in the scratch needs clearing: the partial kernel writes every
+  // element that the reduction then reads.
+  const int chunks = (int)((n + kGramRows - 1) / kGramRows);
+  cudaStream_t st = (cudaStream_t)stream;
+  dim3 grid(ceil_div(p, 32), ceil_div(q, 32), chunks);
+  gram_partial_kernel<<<grid, 256, 0, st>>>(n, p, q, (const double2*)x, ldx, (const double2*)y,
+                                            ldy, (double2*)scratch);
+  const int64_t pq = (int64_t)p * q;
+  gram_reduce_kernel<<<ceil_div(pq, 256), 256, 0, st>>>(chunks, pq, (const double2*)scratch,
+                                                        (double2*)g);
+  count_launches(2);
+  return launch_check(err, cap, "gram_noalloc");
+}

@@ -128,6 +128,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_gram_scratch_bytes": (c_sz, [c_i64, c_i32, c_i32]),
     "aosb_gram": (C.c_int, [c_i64, c_i32, c_i32, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp, c_vp,
                             C.c_char_p, c_sz]),
+    "aosb_gram_noalloc": (C.c_int, [c_i64, c_i32, c_i32, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp,
+                                    C.c_char_p, c_sz]),
     "aosb_dense_mul": (C.c_int, [c_i64, c_i32, c_i32, c_vp, c_i64, c_vp, c_vp, c_i64, c_vp,
                                  C.c_char_p, c_sz]),
     "aosb_column_norms": (C.c_int, [c_i64, c_i32, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp,

@@ -325,6 +325,20 @@ int aosb_gram(int64_t n, int32_t p, int32_t q, const aosb_complex128 *x,
               int64_t ldx, const aosb_complex128 *y, int64_t ldy,
               aosb_complex128 *g, void *scratch, void *stream, char *err,
               size_t err_cap);
+/* aosb_gram without any allocation (no counterpart in the reference).
+ * For callers that cannot allocate device memory when they call: code inside
+ * another framework's memory pool or under a device-memory cap, real-time or
+ * callback contexts where cudaMalloc could block or deadlock, embedders that
+ * must not grow the device heap after start-up.  The partial sums use one
+ * fixed 16 MiB device array inside the library (held on every GPU that
+ * loads it until exit); sizes with ceil(n/512)*p*q*16 bytes above 16 MiB are
+ * rejected with AOSB_ERR_SIZE.  The first call on a device resolves that
+ * array's address with a synchronous runtime call: make it before any stream
+ * capture.  All calls share the one array, so calls that overlap on the GPU
+ * (other streams, other host threads) race; serialise them. */
+int aosb_gram_noalloc(int64_t n, int32_t p, int32_t q, const aosb_complex128 *x,
+                      int64_t ldx, const aosb_complex128 *y, int64_t ldy,
+                      aosb_complex128 *g, void *stream, char *err, size_t err_cap);
 /* y (n x r) = x (n x p) t (p x r), t row-major p x r. */
 int aosb_dense_mul(int64_t n, int32_t p, int32_t r, const aosb_complex128 *x,
                    int64_t ldx, const aosb_complex128 *t, aosb_complex128 *y,
