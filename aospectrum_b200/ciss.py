@@ -91,7 +91,7 @@ class EngineSettings:
     """
 
     precision: str = "mixed"
-    refinement_steps: int = 2
+    refinement_steps: int = 1
     tile: int = 0
     max_pencils: int = 0
     memory_fraction: float = 0.6

@@ -95,8 +95,6 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(int k, const int3
   float* colr = ai + T * LD;      // T  (scratch column)
   float* coli = colr + T;         // T
   int* perm = (int*)(coli + T);   // T
-  __shared__ int s_piv;
-  __shared__ float s_pr, s_pi;
   const int p = blockIdx.x;
   const int tid = threadIdx.x;
   float* g = factor + tile_base(p, n_slots, diag_slot[k], T);
@@ -108,60 +106,113 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(int k, const int3
   for (int r = tid; r < T; r += kDiagThreads) perm[r] = r;
   __syncthreads();
   int bad = 0;
-  // 2D thread layout for the rank-1 update: 16 row lanes x 32 column lanes.
+  // Blocked right-looking LU with partial pivoting (LAPACK getrf order):
+  // warp 0 factors each NB-column panel with warp-level syncs only, then all
+  // threads apply the panel's row interchanges to the other columns, form
+  // U12 = inv(L11) A12 and apply the rank-NB update of the trailing block.
+  constexpr int NB = 8;
+  __shared__ int s_swap[NB];
+  const int warp = tid / 32, lane = tid % 32;
   const int ty = tid / 32, tx = tid % 32;
-  for (int j = 0; j < T; ++j) {
-    if (tid < 32) {
-      float best = -1.0f;
-      int bi = j;
-      for (int r = j + tid; r < T; r += 32) {
-        const float m = fabsf(ar[r * LD + j]) + fabsf(ai[r * LD + j]);
-        if (m > best) { best = m; bi = r; }
-      }
+  for (int j0 = 0; j0 < T; j0 += NB) {
+    if (warp == 0) {
+      for (int j = j0; j < j0 + NB; ++j) {
+        float best = -1.0f;
+        int bi = j;
+        for (int r = j + lane; r < T; r += 32) {
+          const float m = fabsf(ar[r * LD + j]) + fabsf(ai[r * LD + j]);
+          if (m > best) { best = m; bi = r; }
+        }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const float ob = __shfl_down_sync(0xffffffffu, best, o);
-        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-      }
-      if (tid == 0) {
-        s_piv = bi;
-        float pr = ar[bi * LD + j], pi = ai[bi * LD + j];
+        for (int o = 16; o > 0; o >>= 1) {
+          const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        // every lane now holds the same (best, bi)
+        if (bi != j && lane < NB) {
+          const int c = j0 + lane;
+          float t = ar[j * LD + c]; ar[j * LD + c] = ar[bi * LD + c]; ar[bi * LD + c] = t;
+          t = ai[j * LD + c]; ai[j * LD + c] = ai[bi * LD + c]; ai[bi * LD + c] = t;
+        }
+        if (lane == 0) s_swap[j - j0] = bi;
+        __syncwarp();
+        float pr = ar[j * LD + j], pi = ai[j * LD + j];
         float d = pr * pr + pi * pi;
         if (!(d > 0.0f) || !isfinite(d)) {
-          bad = isfinite(d) ? kDevZeroPivot : kDevNonFinite;
+          if (lane == 0) bad = isfinite(d) ? kDevZeroPivot : kDevNonFinite;
           pr = 1.0f; pi = 0.0f; d = 1.0f;
         }
-        s_pr = pr / d;
-        s_pi = -pi / d;
+        __syncwarp();
+        if (lane == 0) { ar[j * LD + j] = pr; ai[j * LD + j] = pi; }
+        const float ipr = pr / d, ipi = -pi / d;
+        for (int r = j + 1 + lane; r < T; r += 32) {
+          const float xr = ar[r * LD + j], xi = ai[r * LD + j];
+          const float lr = xr * ipr - xi * ipi, li = xr * ipi + xi * ipr;
+          ar[r * LD + j] = lr;
+          ai[r * LD + j] = li;
+          // rank-1 update of the remaining panel columns of row r
+          for (int c = j + 1; c < j0 + NB; ++c) {
+            const float ur = ar[j * LD + c], ui = ai[j * LD + c];
+            ar[r * LD + c] -= lr * ur - li * ui;
+            ai[r * LD + c] -= lr * ui + li * ur;
+          }
+        }
+        __syncwarp();
       }
     }
     __syncthreads();
-    const int pv = s_piv;
-    if (pv != j) {
-      for (int c = tid; c < T; c += kDiagThreads) {
-        float t = ar[j * LD + c]; ar[j * LD + c] = ar[pv * LD + c]; ar[pv * LD + c] = t;
-        t = ai[j * LD + c]; ai[j * LD + c] = ai[pv * LD + c]; ai[pv * LD + c] = t;
+    // row interchanges of this panel, applied in order to the other columns
+    for (int c = tid; c < T; c += kDiagThreads) {
+      if (c >= j0 && c < j0 + NB) continue;
+      for (int t = 0; t < NB; ++t) {
+        const int j = j0 + t, bi = s_swap[t];
+        if (bi != j) {
+          float x = ar[j * LD + c]; ar[j * LD + c] = ar[bi * LD + c]; ar[bi * LD + c] = x;
+          x = ai[j * LD + c]; ai[j * LD + c] = ai[bi * LD + c]; ai[bi * LD + c] = x;
+        }
       }
-      if (tid == 0) { int t = perm[j]; perm[j] = perm[pv]; perm[pv] = t; }
-      __syncthreads();
     }
-    if (tid == 0 && bad) { ar[j * LD + j] = 1.0f; ai[j * LD + j] = 0.0f; }
-    const float ipr = s_pr, ipi = s_pi;
-    // scale the column below the pivot
-    for (int r = j + 1 + tid; r < T; r += kDiagThreads) {
-      const float xr = ar[r * LD + j], xi = ai[r * LD + j];
-      ar[r * LD + j] = xr * ipr - xi * ipi;
-      ai[r * LD + j] = xr * ipi + xi * ipr;
+    if (tid == 0) {
+      for (int t = 0; t < NB; ++t) {
+        const int j = j0 + t, bi = s_swap[t];
+        if (bi != j) { int x = perm[j]; perm[j] = perm[bi]; perm[bi] = x; }
+      }
     }
     __syncthreads();
-    // rank-1 update of the trailing block
-    for (int r = j + 1 + ty; r < T; r += kDiagThreads / 32) {
-      const float lr = ar[r * LD + j], li = ai[r * LD + j];
-      for (int c = j + 1 + tx; c < T; c += 32) {
-        const float ur = ar[j * LD + c], ui = ai[j * LD + c];
-        ar[r * LD + c] -= lr * ur - li * ui;
-        ai[r * LD + c] -= lr * ui + li * ur;
+    // U12 = inv(L11) A12: forward substitution down each column c >= j0+NB
+    for (int c = j0 + NB + tid; c < T; c += kDiagThreads) {
+      for (int j = j0 + 1; j < j0 + NB; ++j) {
+        float sr = ar[j * LD + c], si = ai[j * LD + c];
+        for (int q = j0; q < j; ++q) {
+          const float lr = ar[j * LD + q], li = ai[j * LD + q];
+          const float ur = ar[q * LD + c], ui = ai[q * LD + c];
+          sr -= lr * ur - li * ui;
+          si -= lr * ui + li * ur;
+        }
+        ar[j * LD + c] = sr;
+        ai[j * LD + c] = si;
+      }
+    }
+    __syncthreads();
+    // trailing update A22 -= L21 U12 (rank NB)
+    for (int r = j0 + NB + ty; r < T; r += kDiagThreads / 32) {
+      float lr[NB], li[NB];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        lr[q] = ar[r * LD + j0 + q];
+        li[q] = ai[r * LD + j0 + q];
+      }
+      for (int c = j0 + NB + tx; c < T; c += 32) {
+        float sr = ar[r * LD + c], si = ai[r * LD + c];
+#pragma unroll
+        for (int q = 0; q < NB; ++q) {
+          const float ur = ar[(j0 + q) * LD + c], ui = ai[(j0 + q) * LD + c];
+          sr -= lr[q] * ur - li[q] * ui;
+          si -= lr[q] * ui + li[q] * ur;
+        }
+        ar[r * LD + c] = sr;
+        ai[r * LD + c] = si;
       }
     }
     __syncthreads();
@@ -172,7 +223,6 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(int k, const int3
   // lower).  tr/ti hold the b x b temporaries of all pairs of a level.
   float* tr = colr + 2 * T + T;   // after perm (see diag_smem_bytes)
   float* ti = tr + T * T / 2;
-  const int warp = tid / 32, lane = tid % 32;
   // ---- base: 8x8 diagonal blocks, warp w < T/8 takes block w
   if (warp < T / 8) {
     const int b0 = warp * 8;
@@ -326,8 +376,8 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(int k, int nL, int nU,
                                                          const int32_t* __restrict__ pivots) {
   using C = PanelCfg<T>;
   constexpr int S = C::kStrip;
-  constexpr size_t kRaw = sizeof(CgemmSmem<S, T>) > sizeof(CgemmSmem<T, S>)
-                              ? sizeof(CgemmSmem<S, T>) : sizeof(CgemmSmem<T, S>);
+  constexpr size_t kRaw = 2 * (sizeof(CgemmSmem<S, T>) > sizeof(CgemmSmem<T, S>)
+                                   ? sizeof(CgemmSmem<S, T>) : sizeof(CgemmSmem<T, S>));
   __shared__ __align__(16) unsigned char raw[kRaw];
   const int p = blockIdx.y;
   const int item = blockIdx.x / C::kStrips, strip = blockIdx.x % C::kStrips;
@@ -335,7 +385,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(int k, int nL, int nU,
   if (item < nL) {
     // rows [strip*S, +S) of A_ik times inv(U_kk) (upper incl. diagonal)
     constexpr int TM = C::LTM, TN = C::LTN;
-    auto& sm = *reinterpret_cast<CgemmSmem<S, T>*>(raw);
+    auto& sm = *reinterpret_cast<CgemmSmem<S, T>(*)[2]>(raw);
     float* A = factor + tile_base(p, n_slots, lslot[item], T);
     float accr[TM][TN] = {}, acci[TM][TN] = {};
     const int r0 = strip * S;
@@ -360,7 +410,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(int k, int nL, int nU,
   } else if (item < nL + nU) {
     // columns [strip*S, +S) of inv(L_kk) (P_k A_kj)
     constexpr int TM = C::UTM, TN = C::UTN;
-    auto& sm = *reinterpret_cast<CgemmSmem<T, S>*>(raw);
+    auto& sm = *reinterpret_cast<CgemmSmem<T, S>(*)[2]>(raw);
     float* A = factor + tile_base(p, n_slots, uslot[item - nL], T);
     const int32_t* pv = pivots + (size_t)p * n_pad + (size_t)k * T;
     float accr[TM][TN] = {}, acci[TM][TN] = {};
@@ -405,7 +455,7 @@ __global__ void __launch_bounds__(kThreads) schur_kernel(int nU, const int32_t* 
                                                          int64_t n_slots, float* __restrict__ factor) {
   using C = SchurCfg<T>;
   constexpr int BM = C::BM, BN = C::BN, TM = C::TM, TN = C::TN;
-  __shared__ CgemmSmem<BM, BN> sm;
+  __shared__ CgemmSmem<BM, BN> sm[2];
   const int p = blockIdx.y;
   const int pair = blockIdx.x / C::kSub, sub = blockIdx.x % C::kSub;
   const int a = pair / nU, b = pair % nU;

@@ -206,8 +206,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 //                  then C -= acc is stored.
 // Two accumulator sets let the epilogue of one item overlap the MMAs of the
 // next.
-constexpr int kStagesP = 6;
+constexpr int kStagesP = 4;
 constexpr int kEpiWarps = 8;
+constexpr int kXpLd = 36;  // padded row (floats) of the epilogue transposition tile
 constexpr int kPThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemColsP = 512;
 
@@ -220,6 +221,8 @@ struct PShared {
   uint64_t acc_empty[2];
   uint32_t tmem_base;
   int failed;
+  // per epilogue warp: 32 x 32 re and im blocks for the transposition
+  alignas(16) float xp[kEpiWarps][2][32 * kXpLd];
 };
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -338,23 +341,31 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
       }
     }
   } else {
-    // Epilogue warps.
+    // Epilogue warps.  Warp w owns rows 32*(w%4) .. +31 and columns
+    // 64*(w/4) .. +63 of the target tile, processed as two 32 x 32 blocks.
+    // C is read and written coalesced: lane l covers row 4*i + l/8 and
+    // columns 4*(l%8) .. +3 of a block; the accumulator (one row per lane
+    // after tcgen05.ld) is transposed through the warp's padded tile xp.
     const int quarter = warp % 4, half = warp / 4;
-    const int row = quarter * 32 + lane;
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+    const int ro = lane / 8, cg = lane % 8;
+    float* xre = sh.xp[warp][0];
+    float* xim = sh.xp[warp][1];
     int acc = 0;
     uint32_t acc_phase = 0;
     for (int it = blockIdx.x; it < total; it += gridDim.x) {
       const int p = it / n_pairs, pair = it % n_pairs;
       float* C = factor + tile_base(p, n_slots, tslot[pair]);
-      float4* cr = reinterpret_cast<float4*>(C + (size_t)row * kTcT + half * 64);
-      float4* ci = reinterpret_cast<float4*>(C + kTcT * kTcT + (size_t)row * kTcT + half * 64);
-      float4 xr[16], xi[16];
+      // prefetch: 2 blocks x 8 row groups x (re, im)
+      float4 cre[2][8], cim[2][8];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        xr[q] = cr[q];
-        xi[q] = ci[q];
-      }
+      for (int bk = 0; bk < 2; ++bk)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const size_t o = (size_t)(quarter * 32 + 4 * i + ro) * kTcT + half * 64 + bk * 32 + 4 * cg;
+          cre[bk][i] = *reinterpret_cast<const float4*>(C + o);
+          cim[bk][i] = *reinterpret_cast<const float4*>(C + kTcT * kTcT + o);
+        }
       const bool ready = __all_sync(0xffffffffu, mbar_wait(&sh.acc_full[acc], acc_phase) ? 1 : 0);
       if (!ready) {
         if (lane == 0) {
@@ -364,28 +375,50 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t base = tmem + (uint32_t)acc * 256 + (uint32_t)half * 64;
+      const uint32_t base = tmem + (uint32_t)acc * 256 + (uint32_t)half * 64 + lane_addr;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        float vr[16], vi[16];
-        tmem_ld16(base + lane_addr + c * 16, vr);
-        tmem_ld16(base + lane_addr + kTcT + c * 16, vi);
+      for (int bk = 0; bk < 2; ++bk) {
+        float v[16];
+        // real part: columns bk*32 .. +31 of this warp's half
+        tmem_ld16(base + bk * 32, v);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          float4& x = xr[c * 4 + q];
-          float4& y = xi[c * 4 + q];
-          x.x -= vr[4 * q]; x.y -= vr[4 * q + 1]; x.z -= vr[4 * q + 2]; x.w -= vr[4 * q + 3];
-          y.x -= vi[4 * q]; y.y -= vi[4 * q + 1]; y.z -= vi[4 * q + 2]; y.w -= vi[4 * q + 3];
+        for (int j = 0; j < 16; j += 4)
+          *reinterpret_cast<float4*>(xre + lane * kXpLd + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        tmem_ld16(base + bk * 32 + 16, v);
+#pragma unroll
+        for (int j = 0; j < 16; j += 4)
+          *reinterpret_cast<float4*>(xre + lane * kXpLd + 16 + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        tmem_ld16(base + kTcT + bk * 32, v);
+#pragma unroll
+        for (int j = 0; j < 16; j += 4)
+          *reinterpret_cast<float4*>(xim + lane * kXpLd + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        tmem_ld16(base + kTcT + bk * 32 + 16, v);
+#pragma unroll
+        for (int j = 0; j < 16; j += 4)
+          *reinterpret_cast<float4*>(xim + lane * kXpLd + 16 + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float4 ar = *reinterpret_cast<const float4*>(xre + (4 * i + ro) * kXpLd + 4 * cg);
+          const float4 ai = *reinterpret_cast<const float4*>(xim + (4 * i + ro) * kXpLd + 4 * cg);
+          float4& x = cre[bk][i];
+          float4& y = cim[bk][i];
+          x.x -= ar.x; x.y -= ar.y; x.z -= ar.z; x.w -= ar.w;
+          y.x -= ai.x; y.y -= ai.y; y.z -= ai.z; y.w -= ai.w;
         }
+        __syncwarp();
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh.acc_empty[acc]);
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        cr[q] = xr[q];
-        ci[q] = xi[q];
-      }
+      for (int bk = 0; bk < 2; ++bk)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const size_t o = (size_t)(quarter * 32 + 4 * i + ro) * kTcT + half * 64 + bk * 32 + 4 * cg;
+          *reinterpret_cast<float4*>(C + o) = cre[bk][i];
+          *reinterpret_cast<float4*>(C + kTcT * kTcT + o) = cim[bk][i];
+        }
       if (++acc == 2) { acc = 0; acc_phase ^= 1; }
     }
   }

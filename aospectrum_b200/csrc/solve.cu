@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(kThreads) solve_diag_kernel(int k, int nrhs, i
                                                               float2* __restrict__ ytmp) {
   constexpr int BM = 32, BN = 32, TM = 2, TN = 2;
   static_assert((BM / TM) * (BN / TN) == 256, "layout");
-  __shared__ CgemmSmem<BM, BN> sm;
+  __shared__ CgemmSmem<BM, BN> sm[2];
   const int p = blockIdx.z;
   const int c0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
   const float* D = factor + tile_base(p, n_slots, diag_slot[k], T);
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kThreads) solve_diag_kernel(int k, int nrhs, i
     const int row = OP == kLinv ? pv[q] : q;
     return X[(size_t)row * nrhs + col];
   };
-  cgemm_cta<BM, BN, TM, TN>(accr, acci, T, sm, la, lb);
+  cgemm_cta<BM, BN, TM, TN, (OP == kUinvH || OP == kLinvH)>(accr, acci, T, sm, la, lb);
 #pragma unroll
   for (int i = 0; i < TM; ++i)
 #pragma unroll
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kThreads) solve_update_kernel(
   constexpr int TM = BM == 64 ? 4 : 2, TN = 2;
   static_assert((BM / TM) * (BN / TN) == 256, "layout");
   constexpr int kRowBlocks = T / BM;
-  __shared__ CgemmSmem<BM, BN> sm;
+  __shared__ CgemmSmem<BM, BN> sm[2];
   const int p = blockIdx.y;
   const int ncs = (nrhs + BN - 1) / BN;
   const int work_blocks = n_items * kRowBlocks * ncs;
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kThreads) solve_update_kernel(
     if (col >= nrhs) return make_float2(0.f, 0.f);
     return Y[(size_t)q * nrhs + col];
   };
-  cgemm_cta<BM, BN, TM, TN>(accr, acci, T, sm, la, lb);
+  cgemm_cta<BM, BN, TM, TN, OP == kConjT>(accr, acci, T, sm, la, lb);
 #pragma unroll
   for (int a = 0; a < TM; ++a)
 #pragma unroll
@@ -285,6 +285,80 @@ __global__ void shifted_residual_kernel(int64_t n, int nrhs, const int64_t* __re
   }
 }
 
+// Row-block version: rows [rb[b], rb[b+1]) (at most kResRows) share one
+// column pattern (the rows of one atom), so each x row is loaded once per
+// block instead of once per row.  One warp per (block, 32-column strip,
+// pencil); A = H - z S is formed on the fly in FP64.
+constexpr int kResRows = 16;
+
+__global__ void __launch_bounds__(256) shifted_residual_blocks_kernel(
+    int64_t n_blocks, const int32_t* __restrict__ rb, int nrhs,
+    const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+    const float2* __restrict__ hv, const float2* __restrict__ sv, int64_t nnz,
+    const int32_t* __restrict__ pencil_k, const double2* __restrict__ shifts,
+    const double2* __restrict__ b, int64_t b_stride, const double2* __restrict__ x,
+    double2* __restrict__ r, int64_t n) {
+  const int ncs = (nrhs + 31) / 32;
+  const int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const int p = blockIdx.y;
+  if (w >= n_blocks * ncs) return;
+  const int64_t blk = w / ncs;
+  const int c = (int)(w % ncs) * 32 + lane;
+  const int r0 = rb[blk], nr = rb[blk + 1] - rb[blk];
+  const int64_t kp = pencil_k[p];
+  const double2 z = shifts[p];
+  const float2* h = hv + kp * nnz;
+  const float2* s = sv != nullptr ? sv + kp * nnz : nullptr;
+  const double2* xp = x + (size_t)p * n * nrhs;
+  double ar[kResRows], ai[kResRows];
+#pragma unroll
+  for (int q = 0; q < kResRows; ++q) {
+    ar[q] = 0.0;
+    ai[q] = 0.0;
+  }
+  // rows of a block are consecutive with equal lengths: row q starts at
+  // base0 + q * len
+  const int64_t base0 = indptr[r0];
+  const int64_t len = indptr[r0 + 1] - base0;
+  const bool active = c < nrhs;
+  constexpr int U = 4;  // columns whose index and x loads are in flight together
+  for (int64_t e0 = 0; e0 < len; e0 += U) {
+    double2 xv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool ok = e0 + u < len;
+      const int64_t col = ok ? indices[base0 + e0 + u] : 0;
+      xv[u] = (ok && active) ? xp[(size_t)col * nrhs + c] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (e0 + u >= len) break;
+#pragma unroll
+      for (int q = 0; q < kResRows; ++q) {
+        if (q < nr) {
+          const int64_t at = base0 + (int64_t)q * len + e0 + u;
+          const float2 hh = h[at];
+          const float2 ss = s != nullptr ? s[at] : make_float2(0.f, 0.f);
+          const double a_r = (double)hh.x - (z.x * ss.x - z.y * ss.y);
+          const double a_i = (double)hh.y - (z.x * ss.y + z.y * ss.x);
+          ar[q] += a_r * xv[u].x - a_i * xv[u].y;
+          ai[q] += a_r * xv[u].y + a_i * xv[u].x;
+        }
+      }
+    }
+  }
+  if (!active) return;
+#pragma unroll
+  for (int q = 0; q < kResRows; ++q) {
+    if (q < nr) {
+      const int64_t row = r0 + q;
+      const double2 bv = b[(size_t)p * b_stride + (size_t)row * nrhs + c];
+      r[((size_t)p * n + row) * nrhs + c] = make_double2(bv.x - ar[q], bv.y - ai[q]);
+    }
+  }
+}
+
 }  // namespace
 }  // namespace aosb
 
@@ -340,6 +414,29 @@ int aosb_scatter_solution(const aosb_plan_t* P, int32_t np, int32_t nrhs,
       P->n, P->n_pad, nrhs, P->d_pinv, (const float2*)work, (double2*)x, accumulate);
   aosb::count_launches(1);
   return aosb::launch_check(err, cap, "scatter_solution");
+}
+
+int aosb_shifted_residual_blocks(int64_t n, int32_t nrhs, int32_t np, int64_t n_blocks,
+                                 const int32_t* row_blocks, const int64_t* indptr,
+                                 const int32_t* indices, const aosb_complex64* h_values,
+                                 const aosb_complex64* s_values, int64_t nnz,
+                                 const int32_t* pencil_k, const aosb_complex128* shifts,
+                                 const aosb_complex128* b, int64_t b_stride,
+                                 const aosb_complex128* x, aosb_complex128* r, void* stream,
+                                 char* err, size_t cap) {
+  if (row_blocks == nullptr || indptr == nullptr || indices == nullptr || h_values == nullptr ||
+      pencil_k == nullptr || shifts == nullptr || b == nullptr || x == nullptr || r == nullptr)
+    return aosb::set_error(err, cap, AOSB_ERR_NULL, "null argument");
+  if (np <= 0 || np > 65535 || nrhs <= 0 || n <= 0 || n_blocks <= 0)
+    return aosb::set_error(err, cap, AOSB_ERR_BATCH, "invalid batch");
+  const int ncs = (nrhs + 31) / 32;
+  dim3 g(aosb::ceil_div(n_blocks * ncs, 8), np);
+  aosb::shifted_residual_blocks_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(
+      n_blocks, row_blocks, nrhs, indptr, indices, (const float2*)h_values,
+      (const float2*)s_values, nnz, pencil_k, (const double2*)shifts, (const double2*)b,
+      b_stride, (const double2*)x, (double2*)r, n);
+  aosb::count_launches(1);
+  return aosb::launch_check(err, cap, "shifted_residual_blocks");
 }
 
 int aosb_shifted_residual(int64_t n, int32_t nrhs, int32_t np, const int64_t* indptr,

@@ -55,6 +55,28 @@ def _torch():
     return torch
 
 
+def row_blocks(indptr: np.ndarray, indices: np.ndarray, max_rows: int = 16,
+               starts: np.ndarray | None = None) -> np.ndarray:
+    """Start rows of blocks of consecutive rows with identical column sets
+    (at most ``max_rows`` rows each), closed by n.  ``starts`` (e.g. the atom
+    offsets of a bundle) are trusted; otherwise runs are detected."""
+    n = indptr.size - 1
+    if starts is None:
+        lens = np.diff(indptr)
+        same = np.zeros(n, dtype=bool)
+        for r in range(1, n):
+            if lens[r] == lens[r - 1] and np.array_equal(
+                    indices[indptr[r]:indptr[r + 1]], indices[indptr[r - 1]:indptr[r]]):
+                same[r] = True
+        starts = np.flatnonzero(~same)
+    out = []
+    bounds = list(np.asarray(starts, dtype=np.int64)) + [n]
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        out.extend(range(int(a), int(b), max_rows))
+    out.append(n)
+    return np.asarray(out, dtype=np.int32)
+
+
 def choose_tile(n: int) -> int:
     if n <= 256:
         return 32
@@ -293,6 +315,9 @@ class BandEngine:
         if self.settings.search_dimension >= self.n:
             raise SolverError("CISS search dimension must be smaller than matrix dimension")
         self.pattern_seconds = perf_counter() - t0
+        rb = row_blocks(self.pattern.indptr, self.pattern.indices,
+                        starts=None if supervariables is None else supervariables[:-1])
+        self.row_blocks = torch.from_numpy(rb).to(self.device)
         t0 = perf_counter()
         use_tc = self.engine.precision == "mixed" and self.engine.tensor_cores
         tile = self.engine.tile or (128 if use_tc else choose_tile(self.n))
@@ -555,10 +580,23 @@ class BandEngine:
             native.call("aosb_scatter_solution", self.plan.handle, np_, L, wn.data_ptr(),
                         xn.data_ptr(), 1 if it > 0 else 0, st)
             if it < steps:
-                native.call("aosb_shifted_residual", n, L, np_, self.pattern.d_indptr,
-                            self.pattern.d_indices, hvals.data_ptr(), svals.data_ptr(),
-                            self.pattern.nnz, pk.data_ptr(), z.contiguous().data_ptr(),
-                            b.data_ptr(), n * L, xn.data_ptr(), rr.data_ptr(), st)
+                self._residual(n, L, np_, hvals, svals, pk, z, b, xn, rr, st)
+
+    residual_kernel = "rows"   # "rows" or "blocks" (row blocks of one atom)
+
+    def _residual(self, n, L, np_, hvals, svals, pk, z, b, xn, rr, st) -> None:
+        """FP64 r = b - (H - z S) x for every pencil of the batch."""
+        if self.residual_kernel == "blocks":
+            native.call("aosb_shifted_residual_blocks", n, L, np_, self.row_blocks.numel() - 1,
+                        self.row_blocks.data_ptr(), self.pattern.d_indptr,
+                        self.pattern.d_indices, hvals.data_ptr(), svals.data_ptr(),
+                        self.pattern.nnz, pk.data_ptr(), z.contiguous().data_ptr(),
+                        b.data_ptr(), n * L, xn.data_ptr(), rr.data_ptr(), st)
+        else:
+            native.call("aosb_shifted_residual", n, L, np_, self.pattern.d_indptr,
+                        self.pattern.d_indices, hvals.data_ptr(), svals.data_ptr(),
+                        self.pattern.nnz, pk.data_ptr(), z.contiguous().data_ptr(),
+                        b.data_ptr(), n * L, xn.data_ptr(), rr.data_ptr(), st)
 
     def _subspace(self, h, s, mom, interval: EnergyInterval, stages: dict[str, float],
                   nk: int) -> CissResult:

@@ -315,6 +315,8 @@ def main() -> None:
     if rank == 0:
         out["stage_seconds_last_step"] = {k: round(v, 4) for k, v in
                                           stats.get("stage_seconds", {}).items()}
+        out["per_k_stage_seconds"] = {k: round(v, 4) for k, v in
+                                      results[-1][0].stage_seconds.items()}
         # accuracy vs FP64 dense generalized eigenvalues (sampled k points)
         errs = []
         for i in range(min(args.accuracy_kpoints, len(kpts))):

@@ -305,6 +305,20 @@ int aosb_shifted_residual(int64_t n, int32_t n_rhs, int32_t n_pencils,
                           const aosb_complex128 *x, aosb_complex128 *r,
                           void *stream, char *err, size_t err_cap);
 
+/* The same residual for patterns whose rows come in blocks with identical
+ * column sets (the orbitals of one atom): row_blocks[n_blocks+1] (device)
+ * are block start rows, each block at most 16 rows.  Each x row is read
+ * once per block. */
+int aosb_shifted_residual_blocks(int64_t n, int32_t n_rhs, int32_t n_pencils,
+                                 int64_t n_blocks, const int32_t *row_blocks,
+                                 const int64_t *indptr, const int32_t *indices,
+                                 const aosb_complex64 *h_values,
+                                 const aosb_complex64 *s_values, int64_t nnz,
+                                 const int32_t *pencil_k, const aosb_complex128 *shifts,
+                                 const aosb_complex128 *b, int64_t b_stride,
+                                 const aosb_complex128 *x, aosb_complex128 *r,
+                                 void *stream, char *err, size_t err_cap);
+
 /* ------------------------------------------------------------------------
  * FP64 CISS kernels on n x m complex128 blocks (row-major, leading
  * dimension = row stride in elements).

@@ -336,3 +336,40 @@ def test_dropin_solver_classes(golden, torch):
         assert "numeric_factorization" in out.stage_seconds
     finally:
         shifted.close()
+
+
+def test_row_block_residual_matches_per_row(torch):
+    """aosb_shifted_residual_blocks == aosb_shifted_residual (FP64)."""
+    from aospectrum_b200 import native
+    from aospectrum_b200.engine import row_blocks
+
+    b = bundles.small2d()
+    dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[1], torch, 64)
+    try:
+        n, L, P = dev.n, 40, 3
+        dv = torch.device("cuda", 0)
+        rng = np.random.default_rng(9)
+        x = torch.tensor(rng.standard_normal((P, n, L)) + 1j * rng.standard_normal((P, n, L)),
+                         device=dv)
+        bb = torch.tensor(rng.standard_normal((P, n, L)) + 1j * rng.standard_normal((P, n, L)),
+                          device=dv)
+        z = torch.tensor(np.asarray([-2.0 + 0.1j, 0.5 + 0.01j, -1.0 + 1.0j]), device=dv)
+        pk = torch.zeros(P, dtype=torch.int32, device=dv)
+        rb = torch.from_numpy(row_blocks(dev.indptr, dev.indices,
+                                         starts=np.asarray(b.basis.atom_offsets)[:-1])).to(dv)
+        r1 = torch.empty_like(x)
+        r2 = torch.empty_like(x)
+        st = torch.cuda.current_stream().cuda_stream
+        native.call("aosb_shifted_residual", n, L, P, dev.d_indptr, dev.d_indices, h.data_ptr(),
+                    s.data_ptr(), dev.nnz, pk.data_ptr(), z.data_ptr(), bb.data_ptr(), n * L,
+                    x.data_ptr(), r1.data_ptr(), st)
+        native.call("aosb_shifted_residual_blocks", n, L, P, rb.numel() - 1, rb.data_ptr(),
+                    dev.d_indptr, dev.d_indices, h.data_ptr(), s.data_ptr(), dev.nnz,
+                    pk.data_ptr(), z.data_ptr(), bb.data_ptr(), n * L, x.data_ptr(),
+                    r2.data_ptr(), st)
+        torch.cuda.synchronize()
+        a, c = r1.cpu().numpy(), r2.cpu().numpy()
+        assert np.max(np.abs(a - c)) <= 1e-11 * np.max(np.abs(a))
+    finally:
+        dev.close()
+        plan.close()
