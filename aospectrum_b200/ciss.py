@@ -88,6 +88,9 @@ class EngineSettings:
         "natural".
     tensor_cores: with precision "mixed", False keeps the FP32 SIMT tile
         updates (FP32 factor + FP64 refinement + node pairing).
+    tensor_core_panels: with tensor cores, also form the panel tiles
+        L_ik = A_ik inv(U_kk) and U_kj = inv(L_kk) P_k A_kj in split BF16;
+        False keeps them in FP32 SIMT.
     """
 
     precision: str = "mixed"
@@ -97,6 +100,7 @@ class EngineSettings:
     memory_fraction: float = 0.6
     ordering: str = "auto"
     tensor_cores: bool = True
+    tensor_core_panels: bool = True
 
     def __post_init__(self) -> None:
         if self.precision not in PRECISIONS:
@@ -155,11 +159,22 @@ def hermitize(a: np.ndarray) -> np.ndarray:
     return 0.5 * (a + a.conj().T)
 
 
+def small_lapack():
+    """Context that runs host LAPACK on one thread.  The projected problems
+    are at most a few hundred wide; on hosts with many cores a BLAS pool
+    sized to the machine spends far longer waking and synchronising its
+    threads than the factorization itself takes."""
+    from threadpoolctl import threadpool_limits
+
+    return threadpool_limits(limits=1)
+
+
 def truncate_gram(gram: np.ndarray, tolerance: float) -> tuple[np.ndarray, np.ndarray]:
     """Rank truncation of the S-Gram matrix of the moments (reference
     ``_compress_moments``, ciss.py:107-126): returns the transform
     V_keep / sqrt(lambda) and the singular values sqrt(lambda)."""
-    values, vectors = np.linalg.eigh(hermitize(gram))
+    with small_lapack():
+        values, vectors = np.linalg.eigh(hermitize(gram))
     scale = float(np.max(np.abs(values), initial=0.0))
     if scale == 0.0 or not math.isfinite(scale):
         raise SolverError("CISS contour moments have zero numerical rank")
@@ -176,7 +191,8 @@ def projected_eigh(hr: np.ndarray, sr: np.ndarray) -> tuple[np.ndarray, np.ndarr
     from scipy import linalg
 
     try:
-        e, c = linalg.eigh(hermitize(hr), hermitize(sr), check_finite=False, driver="gvd")
+        with small_lapack():
+            e, c = linalg.eigh(hermitize(hr), hermitize(sr), check_finite=False, driver="gvd")
     except linalg.LinAlgError as exc:
         raise SolverError("CISS reduced overlap is not positive definite") from exc
     return e, c

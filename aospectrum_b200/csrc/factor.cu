@@ -567,6 +567,16 @@ int factor_step_panels(const aosb_plan* P, const aosb_factor_args_v1* a, int k, 
   return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "unsupported tile size");
 }
 
+int factor_step_diag(const aosb_plan* P, const aosb_factor_args_v1* a, int k, char* err,
+                     size_t cap) {
+  if (P->T != 128) return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "diagonal step needs tile 128");
+  if (int rc = ensure_diag_attr<128>(err, cap)) return rc;
+  diag_lu_kernel<128><<<a->n_pencils, kDiagThreads, diag_smem_bytes<128>(), (cudaStream_t)a->stream>>>(
+      k, P->d_diag_slot, P->n_slots, P->n_pad, a->factor, a->pivots, a->status);
+  count_launches(1);
+  return 0;
+}
+
 int factor_plain(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
   switch (P->T) {
     case 32: return run_plain<32>(P, a, err, cap);
@@ -600,7 +610,8 @@ int aosb_factor(const aosb_plan_t* plan, const aosb_factor_args_v1* a, char* err
   int rc = aosb::factor_assemble(plan, a, err, cap);
   if (rc) return rc;
   if (a->precision == AOSB_PRECISION_PLAIN) return aosb::factor_plain(plan, a, err, cap);
-  if (a->precision == AOSB_PRECISION_BF16X3) return aosb::factor_tc(plan, a, err, cap);
+  if (a->precision == AOSB_PRECISION_BF16X3 || a->precision == AOSB_PRECISION_BF16X3_FP32_PANELS)
+    return aosb::factor_tc(plan, a, err, cap);
   return set_error(err, cap, AOSB_ERR_ARGUMENT, "unknown precision %d", a->precision);
 }
 

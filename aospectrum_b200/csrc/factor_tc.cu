@@ -10,15 +10,16 @@
 //     K-major, no-swizzle core matrices (8 rows x 16 bytes), cut into 16-wide
 //     K slabs so that one slab of one tile is a single contiguous bulk copy.
 //     For U the operand rows are U's columns (B is K-major).
-//   * schur_tc_kernel: one CTA (4 warps) per (target tile, pencil).  Lane 0
-//     of warp 0 streams slabs with cp.async.bulk into a 3-stage mbarrier
-//     ring; lane 0 of warp 1 issues, per 16-wide K step, 12
-//     tcgen05.mma.kind::f16 (M=128, N=128) into two FP32 TMEM accumulators:
+//   * schur_tc_kernel: persistent and warp specialized (see the kernel).  Per
+//     16-wide K slab the MMA warp issues 12 tcgen05.mma.kind::f16 (M=N=128)
+//     into two FP32 TMEM accumulators:
 //       Re += Lr_h Ur_h + Lr_h Ur_l + Lr_l Ur_h - (Li_h Ui_h + Li_h Ui_l + Li_l Ui_h)
 //       Im += Lr_h Ui_h + Lr_h Ui_l + Lr_l Ui_h + Li_h Ur_h + Li_h Ur_l + Li_l Ur_h
 //     (the minus via the instruction's negate-A bit; lo*lo is dropped).
-//     All four warps then read the accumulators with tcgen05.ld and apply
-//     C -= acc to the FP32 tile in HBM.
+//     The epilogue writes -acc into 128B-swizzled shared tiles and the TMA
+//     unit adds them into the FP32 target tile in L2
+//     (cp.reduce.async.bulk.tensor .add.f32), so C never passes through
+//     the SM's registers.
 //   Every mbarrier wait is bounded; on expiry the CTA records
 //   AOSB_ERR_TIMEOUT in the pencil status, skips the remaining work, and
 //   still frees its TMEM.
@@ -26,9 +27,31 @@
 #include "factor.h"
 #include "cgemm.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <mutex>
+#include <vector>
+
 namespace aosb {
+
+// Optional CUDA-event timing of every schur_tc_kernel launch (on the stream
+// the kernel is launched on), with its algorithmic work: 8 T^3 real flops
+// per (target tile, pencil) and 256 KB of target read + write per target
+// plus one read of each staged operand tile.
+struct SchurTimer {
+  std::mutex mu;
+  bool on = false;
+  std::vector<cudaEvent_t> events;  // start, stop pairs
+  double flops = 0.0, bytes = 0.0;
+  int64_t launches = 0;
+};
+SchurTimer& schur_timer() {
+  static SchurTimer t;
+  return t;
+}
+
 namespace {
 
 constexpr int kTcT = 128;                 // tile edge supported by this path
@@ -52,38 +75,57 @@ __host__ __device__ __forceinline__ uint32_t staged_offset(int row, int k, int p
 }
 
 // ---------------------------------------------------------------------------
-// Staging: blockIdx.x = item (L tiles first, then U tiles), blockIdx.y = pencil.
-__global__ void __launch_bounds__(256) stage_kernel(int nL, int nU, const int32_t* __restrict__ lslot,
-                                                    const int32_t* __restrict__ uslot,
-                                                    int64_t n_slots, const float* __restrict__ factor,
-                                                    unsigned char* __restrict__ staging,
-                                                    int64_t staging_pencil_stride) {
-  const int item = blockIdx.x, p = blockIdx.y;
-  const bool is_l = item < nL;
-  const int slot = is_l ? lslot[item] : uslot[item - nL];
-  const float* F = factor + tile_base(p, n_slots, slot);
-  unsigned char* out = staging + (size_t)p * staging_pencil_stride + (size_t)item * kStagedTileBytes;
+// Staging.  Operand kinds:
+//   A          tile as the A operand (row-major: operand row = tile row,
+//              k = tile column)
+//   B          tile as the B operand (operand row = tile column n, k = tile
+//              row)
+//   B_PERM     B with the tile's rows taken through the pivot order of the
+//              step: k -> row pv[k] (for U_kj = inv(L_kk) P_k A_kj)
+//   A_UNIT_LO  the strictly lower triangle of the diagonal slot with a unit
+//              diagonal and zeros above (inv(L_kk))
+//   B_UPPER    the upper triangle (with diagonal) of the diagonal slot and
+//              zeros below (inv(U_kk))
+enum StageKind : int { kStageA = 0, kStageB = 1, kStageBPerm = 2, kStageAUnitLower = 3, kStageBUpper = 4 };
+
+__device__ __forceinline__ void stage_tile(const float* __restrict__ F, unsigned char* __restrict__ out,
+                                           int kind, const int32_t* __restrict__ pv) {
+  const bool a_side = kind == kStageA || kind == kStageAUnitLower;
   // Each thread converts pairs of consecutive k for one operand row, so a
   // 4-byte store writes two BF16 values.
   for (int e = threadIdx.x; e < kTcT * (kTcT / 2); e += blockDim.x) {
     int row, k;
-    float r0, i0, r1, i1;
-    if (is_l) {
-      // A = L (row-major): operand row = tile row, k = tile column
+    float re[2], im[2];
+    if (a_side) {
       row = e / (kTcT / 2);
       k = (e % (kTcT / 2)) * 2;
       const size_t o = (size_t)row * kTcT + k;
-      r0 = F[o]; r1 = F[o + 1];
-      i0 = F[o + kTcT * kTcT]; i1 = F[o + 1 + kTcT * kTcT];
+      re[0] = F[o]; re[1] = F[o + 1];
+      im[0] = F[o + kTcT * kTcT]; im[1] = F[o + 1 + kTcT * kTcT];
+      if (kind == kStageAUnitLower) {
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const int q = k + t;
+          if (q >= row) {
+            re[t] = q == row ? 1.0f : 0.0f;
+            im[t] = 0.0f;
+          }
+        }
+      }
     } else {
-      // B = U (row-major, k x n): operand row = column n, k = tile row
       k = (e / kTcT) * 2;
       row = e % kTcT;
-      const size_t o0 = (size_t)k * kTcT + row, o1 = (size_t)(k + 1) * kTcT + row;
-      r0 = F[o0]; r1 = F[o1];
-      i0 = F[o0 + kTcT * kTcT]; i1 = F[o1 + kTcT * kTcT];
+      const int q0 = kind == kStageBPerm ? pv[k] : k;
+      const int q1 = kind == kStageBPerm ? pv[k + 1] : k + 1;
+      const size_t o0 = (size_t)q0 * kTcT + row, o1 = (size_t)q1 * kTcT + row;
+      re[0] = F[o0]; re[1] = F[o1];
+      im[0] = F[o0 + kTcT * kTcT]; im[1] = F[o1 + kTcT * kTcT];
+      if (kind == kStageBUpper) {
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+          if (k + t > row) re[t] = im[t] = 0.0f;
+      }
     }
-    const float re[2] = {r0, r1}, im[2] = {i0, i1};
     __nv_bfloat162 plane[4];
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
@@ -101,6 +143,37 @@ __global__ void __launch_bounds__(256) stage_kernel(int nL, int nU, const int32_
     for (int pl = 0; pl < 4; ++pl)
       *reinterpret_cast<__nv_bfloat162*>(out + staged_offset(row, k, pl)) = plane[pl];
   }
+}
+
+// blockIdx.x = item, blockIdx.y = pencil.
+//   Schur staging (panel == 0): items [0, nL) = L_ik as A, [nL, nL+nU) =
+//     U_kj as B.
+//   Panel staging (panel == 1): items [0, nL) = A_ik as A, [nL, nL+nU) =
+//     P_k A_kj as B, nL+nU = inv(L_kk) as A, nL+nU+1 = inv(U_kk) as B.
+__global__ void __launch_bounds__(256) stage_kernel(int nL, int nU, int panel, int k,
+                                                    const int32_t* __restrict__ lslot,
+                                                    const int32_t* __restrict__ uslot, int diag_slot,
+                                                    int64_t n_slots, int64_t n_pad,
+                                                    const float* __restrict__ factor,
+                                                    const int32_t* __restrict__ pivots,
+                                                    unsigned char* __restrict__ staging,
+                                                    int64_t staging_pencil_stride) {
+  const int item = blockIdx.x, p = blockIdx.y;
+  int slot, kind;
+  if (item < nL) {
+    slot = lslot[item];
+    kind = kStageA;
+  } else if (item < nL + nU) {
+    slot = uslot[item - nL];
+    kind = panel ? kStageBPerm : kStageB;
+  } else {
+    slot = diag_slot;
+    kind = item == nL + nU ? kStageAUnitLower : kStageBUpper;
+  }
+  const float* F = factor + tile_base(p, n_slots, slot);
+  const int32_t* pv = pivots + (size_t)p * n_pad + (size_t)k * kTcT;
+  unsigned char* out = staging + (size_t)p * staging_pencil_stride + (size_t)item * kStagedTileBytes;
+  stage_tile(F, out, kind, pv);
 }
 
 // ---------------------------------------------------------------------------
@@ -181,6 +254,31 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                : "memory");
 }
 
+// C[box at (x, y)] += smem tile (FP32 add in L2), one bulk group per commit.
+__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, const void* src, int x,
+                                                  int y) {
+  asm volatile(
+      "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(smem_u32(src)), "r"(x), "r"(y)
+      : "memory");
+}
+// C[box at (x, y)] = smem tile.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(smem_u32(src)), "r"(x), "r"(y)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
   asm volatile(
@@ -201,14 +299,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 //                  kStages-deep ring (cp.async.bulk + mbarrier complete_tx);
 //   warp 9 lane 0  MMA issuer: 12 tcgen05.mma per slab into accumulator set
 //                  acc (TMEM columns acc*256 + [0,128) real, +[128,256) imag);
-//   warps 0-7      epilogue: C rows 32*(w%4) + lane, columns 64*(w/4) ..+63;
-//                  the C values are loaded before the accumulator is ready,
-//                  then C -= acc is stored.
+//   warps 0-7      epilogue: rows 32*(w%4) .. +31 (TMEM lanes), columns
+//                  64*(w/4) .. +63 as two 32 x 32 blocks; each block's -acc
+//                  goes through the warp's swizzled shared tile into a TMA
+//                  reduce-add on the target tile.
 // Two accumulator sets let the epilogue of one item overlap the MMAs of the
 // next.
 constexpr int kStagesP = 4;
 constexpr int kEpiWarps = 8;
-constexpr int kXpLd = 36;  // padded row (floats) of the epilogue transposition tile
 constexpr int kPThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemColsP = 512;
 
@@ -221,18 +319,52 @@ struct PShared {
   uint64_t acc_empty[2];
   uint32_t tmem_base;
   int failed;
-  // per epilogue warp: 32 x 32 re and im blocks for the transposition
-  alignas(16) float xp[kEpiWarps][2][32 * kXpLd];
+  // per epilogue warp: one 32 x 32 block of -acc (re, im planes), laid out
+  // as the TMA 128-byte swizzle expects (row r at r * 128 bytes, 16-byte
+  // chunk c of the row at chunk position c ^ (r % 8))
+  alignas(1024) float ep[kEpiWarps][2][32 * 32];
 };
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// Work item -> (staged A index, staged B index, target slot).
+//   Schur (panel == 0): pair = a * nU + b over the step's L x U tiles; the
+//     target gets C -= A B (TMA reduce-add of -acc).
+//   Panel (panel == 1): pair < nL: L_ik = A_ik inv(U_kk); else
+//     U_kj = inv(L_kk) P_k A_kj; the target is overwritten with A B (TMA
+//     store of acc).
+struct ItemMap {
+  int panel, nL, nU, n_pairs;
+  const int32_t* tslot;  // Schur targets [nL * nU]
+  const int32_t* lslot;  // panel L targets [nL]
+  const int32_t* uslot;  // panel U targets [nU]
+};
+
+__device__ __forceinline__ void item_operands(const ItemMap& m, int pair, int& ia, int& ib) {
+  if (!m.panel) {
+    ia = pair / m.nU;
+    ib = m.nL + pair % m.nU;
+  } else if (pair < m.nL) {
+    ia = pair;
+    ib = m.nL + m.nU + 1;
+  } else {
+    ia = m.nL + m.nU;
+    ib = pair;
+  }
+}
+
+__device__ __forceinline__ int item_target(const ItemMap& m, int pair) {
+  if (!m.panel) return m.tslot[pair];
+  return pair < m.nL ? m.lslot[pair] : m.uslot[pair - m.nL];
+}
+
 __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
-    int nU, int step_items, int n_pairs, int n_pencils, const int32_t* __restrict__ tslot,
-    int64_t n_slots, float* __restrict__ factor, const unsigned char* __restrict__ staging,
-    int64_t staging_pencil_stride, int32_t* __restrict__ status) {
+    const ItemMap map, int n_pencils, int64_t n_slots, const unsigned char* __restrict__ staging,
+    int64_t staging_pencil_stride, int32_t* __restrict__ status,
+    const __grid_constant__ CUtensorMap tmap_c) {
+  const int n_pairs = map.n_pairs;
   extern __shared__ unsigned char dyn[];
   PShared& sh = *reinterpret_cast<PShared*>(
       (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
@@ -267,10 +399,12 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
       uint32_t phase = 0;
       for (int it = blockIdx.x; it < total && !sh.failed; it += gridDim.x) {
         const int p = it / n_pairs, pair = it % n_pairs;
+        int ia, ib;
+        item_operands(map, pair, ia, ib);
         const unsigned char* stA = staging + (size_t)p * staging_pencil_stride +
-                                   (size_t)(pair / nU) * kStagedTileBytes;
+                                   (size_t)ia * kStagedTileBytes;
         const unsigned char* stB = staging + (size_t)p * staging_pencil_stride +
-                                   (size_t)(step_items + pair % nU) * kStagedTileBytes;
+                                   (size_t)ib * kStagedTileBytes;
         for (int s = 0; s < kSlabs; ++s) {
           if (!mbar_wait(&sh.empty[stage], phase ^ 1)) {
             sh.failed = 1;
@@ -341,31 +475,24 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
       }
     }
   } else {
-    // Epilogue warps.  Warp w owns rows 32*(w%4) .. +31 and columns
-    // 64*(w/4) .. +63 of the target tile, processed as two 32 x 32 blocks.
-    // C is read and written coalesced: lane l covers row 4*i + l/8 and
-    // columns 4*(l%8) .. +3 of a block; the accumulator (one row per lane
-    // after tcgen05.ld) is transposed through the warp's padded tile xp.
+    // Epilogue warps.  Warp w owns TMEM lanes (tile rows) 32*(w%4) .. +31
+    // and columns 64*(w/4) .. +63, as two 32 x 32 blocks.  Lane l holds row
+    // l of a block after tcgen05.ld; it writes the negated values into the
+    // warp's swizzled shared tile, and lane 0 hands the tile to the TMA
+    // unit, which adds it into the target tile (C -= acc).  The tile is
+    // rewritten only after the previous reduce has finished reading it.
     const int quarter = warp % 4, half = warp / 4;
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
-    const int ro = lane / 8, cg = lane % 8;
-    float* xre = sh.xp[warp][0];
-    float* xim = sh.xp[warp][1];
+    float* bre = sh.ep[warp][0];
+    float* bim = sh.ep[warp][1];
+    const int sw = lane & 7;
+    const float sgn = map.panel ? 1.0f : -1.0f;  // store acc / add -acc
     int acc = 0;
     uint32_t acc_phase = 0;
     for (int it = blockIdx.x; it < total; it += gridDim.x) {
       const int p = it / n_pairs, pair = it % n_pairs;
-      float* C = factor + tile_base(p, n_slots, tslot[pair]);
-      // prefetch: 2 blocks x 8 row groups x (re, im)
-      float4 cre[2][8], cim[2][8];
-#pragma unroll
-      for (int bk = 0; bk < 2; ++bk)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const size_t o = (size_t)(quarter * 32 + 4 * i + ro) * kTcT + half * 64 + bk * 32 + 4 * cg;
-          cre[bk][i] = *reinterpret_cast<const float4*>(C + o);
-          cim[bk][i] = *reinterpret_cast<const float4*>(C + kTcT * kTcT + o);
-        }
+      // first row of the target tile's real plane in the [rows][128] view
+      const int64_t row0 = ((int64_t)p * n_slots + item_target(map, pair)) * (2 * kTcT);
       const bool ready = __all_sync(0xffffffffu, mbar_wait(&sh.acc_full[acc], acc_phase) ? 1 : 0);
       if (!ready) {
         if (lane == 0) {
@@ -378,49 +505,48 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
       const uint32_t base = tmem + (uint32_t)acc * 256 + (uint32_t)half * 64 + lane_addr;
 #pragma unroll
       for (int bk = 0; bk < 2; ++bk) {
-        float v[16];
-        // real part: columns bk*32 .. +31 of this warp's half
-        tmem_ld16(base + bk * 32, v);
-#pragma unroll
-        for (int j = 0; j < 16; j += 4)
-          *reinterpret_cast<float4*>(xre + lane * kXpLd + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-        tmem_ld16(base + bk * 32 + 16, v);
-#pragma unroll
-        for (int j = 0; j < 16; j += 4)
-          *reinterpret_cast<float4*>(xre + lane * kXpLd + 16 + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-        tmem_ld16(base + kTcT + bk * 32, v);
-#pragma unroll
-        for (int j = 0; j < 16; j += 4)
-          *reinterpret_cast<float4*>(xim + lane * kXpLd + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-        tmem_ld16(base + kTcT + bk * 32 + 16, v);
-#pragma unroll
-        for (int j = 0; j < 16; j += 4)
-          *reinterpret_cast<float4*>(xim + lane * kXpLd + 16 + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-        __syncwarp();
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const float4 ar = *reinterpret_cast<const float4*>(xre + (4 * i + ro) * kXpLd + 4 * cg);
-          const float4 ai = *reinterpret_cast<const float4*>(xim + (4 * i + ro) * kXpLd + 4 * cg);
-          float4& x = cre[bk][i];
-          float4& y = cim[bk][i];
-          x.x -= ar.x; x.y -= ar.y; x.z -= ar.z; x.w -= ar.w;
-          y.x -= ai.x; y.y -= ai.y; y.z -= ai.z; y.w -= ai.w;
+        float vr[2][16], vi[2][16];
+        tmem_ld16(base + bk * 32, vr[0]);
+        tmem_ld16(base + bk * 32 + 16, vr[1]);
+        tmem_ld16(base + kTcT + bk * 32, vi[0]);
+        tmem_ld16(base + kTcT + bk * 32 + 16, vi[1]);
+        if (bk == 1) {
+          // every TMEM read of this accumulator is done: release it
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sh.acc_empty[acc]);
         }
+        if (lane == 0) bulk_wait_read_all();
         __syncwarp();
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const int h = c / 4, j = (c % 4) * 4;
+          const int off = lane * 32 + ((c ^ sw) * 4);
+          *reinterpret_cast<float4*>(bre + off) = make_float4(
+              sgn * vr[h][j], sgn * vr[h][j + 1], sgn * vr[h][j + 2], sgn * vr[h][j + 3]);
+          *reinterpret_cast<float4*>(bim + off) = make_float4(
+              sgn * vi[h][j], sgn * vi[h][j + 1], sgn * vi[h][j + 2], sgn * vi[h][j + 3]);
+        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          const int x = half * 64 + bk * 32;
+          const int y = (int)(row0 + quarter * 32);
+          if (map.panel) {
+            tma_store_2d(&tmap_c, bre, x, y);
+            tma_store_2d(&tmap_c, bim, x, y + kTcT);
+          } else {
+            tma_reduce_add_2d(&tmap_c, bre, x, y);
+            tma_reduce_add_2d(&tmap_c, bim, x, y + kTcT);
+          }
+          bulk_commit();
+        }
       }
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&sh.acc_empty[acc]);
-#pragma unroll
-      for (int bk = 0; bk < 2; ++bk)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const size_t o = (size_t)(quarter * 32 + 4 * i + ro) * kTcT + half * 64 + bk * 32 + 4 * cg;
-          *reinterpret_cast<float4*>(C + o) = cre[bk][i];
-          *reinterpret_cast<float4*>(C + kTcT * kTcT + o) = cim[bk][i];
-        }
       if (++acc == 2) { acc = 0; acc_phase ^= 1; }
     }
+    // the target updates must be complete (not only read) before exit
+    if (lane == 0) bulk_wait_all();
+    __syncwarp();
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -433,14 +559,51 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
 
 }  // namespace
 
-size_t factor_tc_workspace(const aosb_plan* P, int32_t n_pencils) {
-  if (P->T != kTcT) return 0;
+static int64_t staged_tiles_per_pencil(const aosb_plan* P) {
   int64_t most = 0;
   for (int64_t k = 0; k < P->nb; ++k) {
     const int64_t items = (P->lb_off[k + 1] - P->lb_off[k]) + (P->ur_off[k + 1] - P->ur_off[k]);
     most = items > most ? items : most;
   }
-  return (size_t)(most > 0 ? most : 1) * kStagedTileBytes * (size_t)n_pencils;
+  return most + 2;
+}
+
+size_t factor_tc_workspace(const aosb_plan* P, int32_t n_pencils) {
+  if (P->T != kTcT) return 0;
+  return (size_t)staged_tiles_per_pencil(P) * kStagedTileBytes * (size_t)n_pencils;
+}
+
+// Tensor map of the factor storage as a [rows][T] FP32 matrix (each tile is
+// 2 planes x T rows), 32 x 32 boxes, 128-byte swizzle: the destination of
+// the epilogue's bulk reduce-add.
+static int factor_tensor_map(void* factor, int64_t rows, CUtensorMap* map, char* err, size_t cap) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (encode == nullptr) {
+      cudaDriverEntryPointQueryResult q;
+      void* fn = nullptr;
+      cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+      if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || fn == nullptr)
+        return set_error(err, cap, AOSB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+      encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+  }
+  if (((uintptr_t)factor & 15) != 0)
+    return set_error(err, cap, AOSB_ERR_ARGUMENT, "factor storage must be 16-byte aligned");
+  if (rows <= 0 || rows > (int64_t)INT32_MAX)
+    return set_error(err, cap, AOSB_ERR_SIZE, "factor storage too large for 32-bit TMA rows");
+  cuuint64_t gdim[2] = {(cuuint64_t)kTcT, (cuuint64_t)rows};
+  cuuint64_t gstride[1] = {(cuuint64_t)kTcT * sizeof(float)};
+  cuuint32_t box[2] = {32, 32};
+  cuuint32_t estride[2] = {1, 1};
+  CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, factor, gdim, gstride, box, estride,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(err, cap, AOSB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return 0;
 }
 
 int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
@@ -463,32 +626,101 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   int device = 0, sms = 148;
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  int64_t most = 0;
-  for (int64_t k = 0; k < P->nb; ++k) {
-    const int64_t items = (P->lb_off[k + 1] - P->lb_off[k]) + (P->ur_off[k + 1] - P->ur_off[k]);
-    most = items > most ? items : most;
-  }
-  const int64_t pencil_stride = (most > 0 ? most : 1) * (int64_t)kStagedTileBytes;
+  // staged tiles per pencil: the step's L and U tiles plus the two
+  // diagonal inverses of the panel product
+  const int64_t pencil_stride = staged_tiles_per_pencil(P) * (int64_t)kStagedTileBytes;
   unsigned char* staging = (unsigned char*)a->workspace;
+  CUtensorMap tmap_c;
+  if (int rc = factor_tensor_map(a->factor, (int64_t)np * P->n_slots * 2 * kTcT, &tmap_c, err, cap))
+    return rc;
+  const bool tc_panels = a->precision != AOSB_PRECISION_BF16X3_FP32_PANELS;
+  auto grid_for = [&](int64_t items) { return (int)(items < sms ? items : sms); };
   for (int64_t k = 0; k < P->nb; ++k) {
-    int rc = factor_step_panels(P, a, (int)k, err, cap);
-    if (rc) return rc;
     const int nL = P->lb_off[k + 1] - P->lb_off[k];
     const int nU = P->ur_off[k + 1] - P->ur_off[k];
+    const int32_t* lslot = P->d_lb_slot + P->lb_off[k];
+    const int32_t* uslot = P->d_ur_slot + P->ur_off[k];
+    if (!tc_panels) {
+      if (int rc = factor_step_panels(P, a, (int)k, err, cap)) return rc;
+    } else {
+      if (int rc = factor_step_diag(P, a, (int)k, err, cap)) return rc;
+      if (nL + nU > 0) {
+        // L_ik = A_ik inv(U_kk), U_kj = inv(L_kk) P_k A_kj on the tensor cores
+        stage_kernel<<<dim3(nL + nU + 2, np), 256, 0, st>>>(
+            nL, nU, 1, (int)k, lslot, uslot, P->diag_slot[k], P->n_slots, P->n_pad, a->factor,
+            a->pivots, staging, pencil_stride);
+        const ItemMap pm{1, nL, nU, nL + nU, nullptr, lslot, uslot};
+        schur_tc_kernel<<<grid_for((int64_t)(nL + nU) * np), kPThreads, smem, st>>>(
+            pm, np, P->n_slots, staging, pencil_stride, a->status, tmap_c);
+        count_launches(2);
+      }
+    }
     if (nL == 0 || nU == 0) continue;
-    stage_kernel<<<dim3(nL + nU, np), 256, 0, st>>>(nL, nU, P->d_lb_slot + P->lb_off[k],
-                                                   P->d_ur_slot + P->ur_off[k], P->n_slots,
-                                                   a->factor, staging, pencil_stride);
+    stage_kernel<<<dim3(nL + nU, np), 256, 0, st>>>(nL, nU, 0, (int)k, lslot, uslot, 0, P->n_slots,
+                                                   P->n_pad, a->factor, a->pivots, staging,
+                                                   pencil_stride);
     const int64_t items = (int64_t)nL * nU * np;
     if ((int64_t)nL * nU > INT32_MAX / 65536)
       return set_error(err, cap, AOSB_ERR_SIZE, "too many Schur targets in one step");
-    const int grid = (int)(items < sms ? items : sms);
-    schur_tc_kernel<<<grid, kPThreads, smem, st>>>(nU, nL, nL * nU, np, P->d_sc_slot + P->sc_off[k],
-                                                   P->n_slots, a->factor, staging, pencil_stride,
-                                                   a->status);
+    const int grid = grid_for(items);
+    SchurTimer& tm = schur_timer();
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    {
+      std::lock_guard<std::mutex> lock(tm.mu);
+      if (tm.on && cudaEventCreate(&ev[0]) == cudaSuccess && cudaEventCreate(&ev[1]) == cudaSuccess) {
+        cudaEventRecord(ev[0], st);
+      } else {
+        if (ev[0]) cudaEventDestroy(ev[0]);
+        ev[0] = ev[1] = nullptr;
+      }
+    }
+    const ItemMap sm{0, nL, nU, nL * nU, P->d_sc_slot + P->sc_off[k], nullptr, nullptr};
+    schur_tc_kernel<<<grid, kPThreads, smem, st>>>(sm, np, P->n_slots, staging, pencil_stride,
+                                                   a->status, tmap_c);
     count_launches(2);
+    if (ev[0] != nullptr) {
+      cudaEventRecord(ev[1], st);
+      std::lock_guard<std::mutex> lock(tm.mu);
+      tm.events.push_back(ev[0]);
+      tm.events.push_back(ev[1]);
+      tm.flops += (double)items * 8.0 * kTcT * kTcT * kTcT;
+      tm.bytes += (double)items * 2.0 * 2 * kTcT * kTcT * sizeof(float) +
+                  (double)(nL + nU) * np * kStagedTileBytes;
+      tm.launches += 1;
+    }
   }
   return launch_check(err, cap, "tensor-core factorization");
 }
 
 }  // namespace aosb
+
+extern "C" int aosb_kernel_timing(int32_t enable) {
+  aosb::SchurTimer& t = aosb::schur_timer();
+  std::lock_guard<std::mutex> lock(t.mu);
+  for (cudaEvent_t e : t.events) cudaEventDestroy(e);
+  t.events.clear();
+  t.flops = t.bytes = 0.0;
+  t.launches = 0;
+  t.on = enable != 0;
+  return 0;
+}
+
+extern "C" int aosb_kernel_timing_read(double* total_ms, double* flops, double* bytes,
+                                       int64_t* launches) {
+  aosb::SchurTimer& t = aosb::schur_timer();
+  std::lock_guard<std::mutex> lock(t.mu);
+  double ms = 0.0;
+  for (size_t i = 0; i + 1 < t.events.size(); i += 2) {
+    if (cudaEventSynchronize(t.events[i + 1]) != cudaSuccess) return AOSB_ERR_CUDA;
+    float one = 0.0f;
+    if (cudaEventElapsedTime(&one, t.events[i], t.events[i + 1]) != cudaSuccess)
+      return AOSB_ERR_CUDA;
+    ms += one;
+  }
+  if (total_ms) *total_ms = ms;
+  if (flops) *flops = t.flops;
+  if (bytes) *bytes = t.bytes;
+  if (launches) *launches = t.launches;
+  return 0;
+}
+

@@ -286,76 +286,112 @@ __global__ void shifted_residual_kernel(int64_t n, int nrhs, const int64_t* __re
 }
 
 // Row-block version: rows [rb[b], rb[b+1]) (at most kResRows) share one
-// column pattern (the rows of one atom), so each x row is loaded once per
-// block instead of once per row.  One warp per (block, 32-column strip,
-// pencil); A = H - z S is formed on the fly in FP64.
+// column pattern (the rows of one atom).  One CTA of kResWarps warps per
+// (block, 32-column strip, pencil); the warps split the block's columns.
+// Per chunk of 32 columns each lane forms A = H - z S in FP64 for one
+// column and every row of the block into shared memory (so A is formed
+// once, not once per lane); then every lane walks the chunk, loading each
+// x row once for all rows of the block.  Partial sums of the warps are
+// added in shared memory.
 constexpr int kResRows = 16;
+constexpr int kResWarps = 4;
 
-__global__ void __launch_bounds__(256) shifted_residual_blocks_kernel(
+__global__ void __launch_bounds__(kResWarps * 32) shifted_residual_blocks_kernel(
     int64_t n_blocks, const int32_t* __restrict__ rb, int nrhs,
     const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const float2* __restrict__ hv, const float2* __restrict__ sv, int64_t nnz,
     const int32_t* __restrict__ pencil_k, const double2* __restrict__ shifts,
     const double2* __restrict__ b, int64_t b_stride, const double2* __restrict__ x,
     double2* __restrict__ r, int64_t n) {
+  __shared__ double2 as[kResWarps][kResRows][32];
+  __shared__ int32_t cs[kResWarps][32];
   const int ncs = (nrhs + 31) / 32;
-  const int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
+  const int64_t blk = blockIdx.x / ncs;
+  const int c = (int)(blockIdx.x % ncs) * 32 + (threadIdx.x & 31);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.y;
-  if (w >= n_blocks * ncs) return;
-  const int64_t blk = w / ncs;
-  const int c = (int)(w % ncs) * 32 + lane;
+  if (blk >= n_blocks) return;
   const int r0 = rb[blk], nr = rb[blk + 1] - rb[blk];
   const int64_t kp = pencil_k[p];
   const double2 z = shifts[p];
   const float2* h = hv + kp * nnz;
   const float2* s = sv != nullptr ? sv + kp * nnz : nullptr;
   const double2* xp = x + (size_t)p * n * nrhs;
+  const bool active = c < nrhs;
+  // rows of a block are consecutive with equal lengths: row q starts at
+  // base0 + q * len
+  const int64_t base0 = indptr[r0];
+  const int64_t len = indptr[r0 + 1] - base0;
+  const int64_t per = (len + kResWarps - 1) / kResWarps;
+  const int64_t w0 = (int64_t)warp * per;
+  const int64_t w1 = w0 + per < len ? w0 + per : len;
   double ar[kResRows], ai[kResRows];
 #pragma unroll
   for (int q = 0; q < kResRows; ++q) {
     ar[q] = 0.0;
     ai[q] = 0.0;
   }
-  // rows of a block are consecutive with equal lengths: row q starts at
-  // base0 + q * len
-  const int64_t base0 = indptr[r0];
-  const int64_t len = indptr[r0 + 1] - base0;
-  const bool active = c < nrhs;
-  constexpr int U = 4;  // columns whose index and x loads are in flight together
-  for (int64_t e0 = 0; e0 < len; e0 += U) {
-    double2 xv[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const bool ok = e0 + u < len;
-      const int64_t col = ok ? indices[base0 + e0 + u] : 0;
-      xv[u] = (ok && active) ? xp[(size_t)col * nrhs + c] : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (e0 + u >= len) break;
+  for (int64_t e0 = w0; e0 < w1; e0 += 32) {
+    const int cnt = (int)(w1 - e0 < 32 ? w1 - e0 : 32);
+    if (lane < cnt) {
+      cs[warp][lane] = indices[base0 + e0 + lane];
 #pragma unroll
       for (int q = 0; q < kResRows; ++q) {
         if (q < nr) {
-          const int64_t at = base0 + (int64_t)q * len + e0 + u;
+          const int64_t at = base0 + (int64_t)q * len + e0 + lane;
           const float2 hh = h[at];
           const float2 ss = s != nullptr ? s[at] : make_float2(0.f, 0.f);
-          const double a_r = (double)hh.x - (z.x * ss.x - z.y * ss.y);
-          const double a_i = (double)hh.y - (z.x * ss.y + z.y * ss.x);
-          ar[q] += a_r * xv[u].x - a_i * xv[u].y;
-          ai[q] += a_r * xv[u].y + a_i * xv[u].x;
+          as[warp][q][lane] = make_double2((double)hh.x - (z.x * ss.x - z.y * ss.y),
+                                           (double)hh.y - (z.x * ss.y + z.y * ss.x));
         }
       }
     }
-  }
-  if (!active) return;
+    __syncwarp();
+    constexpr int U = 4;  // x rows in flight together
+    for (int j0 = 0; j0 < cnt; j0 += U) {
+      double2 xv[U];
 #pragma unroll
-  for (int q = 0; q < kResRows; ++q) {
-    if (q < nr) {
-      const int64_t row = r0 + q;
-      const double2 bv = b[(size_t)p * b_stride + (size_t)row * nrhs + c];
-      r[((size_t)p * n + row) * nrhs + c] = make_double2(bv.x - ar[q], bv.y - ai[q]);
+      for (int u = 0; u < U; ++u)
+        xv[u] = (j0 + u < cnt && active) ? xp[(size_t)cs[warp][j0 + u] * nrhs + c]
+                                         : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (j0 + u >= cnt) break;
+#pragma unroll
+        for (int q = 0; q < kResRows; ++q) {
+          if (q < nr) {
+            const double2 a = as[warp][q][j0 + u];
+            ar[q] += a.x * xv[u].x - a.y * xv[u].y;
+            ai[q] += a.x * xv[u].y + a.y * xv[u].x;
+          }
+        }
+      }
     }
+    __syncwarp();
+  }
+  // cross-warp sum: reuse `as` as [warp][row][lane]
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < kResRows; ++q)
+    if (q < nr) as[warp][q][lane] = make_double2(ar[q], ai[q]);
+  __syncthreads();
+  if (!active) return;
+  for (int q = warp; q < nr; q += kResWarps) {
+    const int64_t row = r0 + q;
+    if (q >= kResRows) {
+      // blocks longer than kResRows break the contract: poison those rows
+      r[((size_t)p * n + row) * nrhs + c] = make_double2(__longlong_as_double(0x7ff8000000000000ll),
+                                                         __longlong_as_double(0x7ff8000000000000ll));
+      continue;
+    }
+    double sr = 0.0, si = 0.0;
+#pragma unroll
+    for (int w = 0; w < kResWarps; ++w) {
+      sr += as[w][q][lane].x;
+      si += as[w][q][lane].y;
+    }
+    const double2 bv = b[(size_t)p * b_stride + (size_t)row * nrhs + c];
+    r[((size_t)p * n + row) * nrhs + c] = make_double2(bv.x - sr, bv.y - si);
   }
 }
 
@@ -430,8 +466,9 @@ int aosb_shifted_residual_blocks(int64_t n, int32_t nrhs, int32_t np, int64_t n_
   if (np <= 0 || np > 65535 || nrhs <= 0 || n <= 0 || n_blocks <= 0)
     return aosb::set_error(err, cap, AOSB_ERR_BATCH, "invalid batch");
   const int ncs = (nrhs + 31) / 32;
-  dim3 g(aosb::ceil_div(n_blocks * ncs, 8), np);
-  aosb::shifted_residual_blocks_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(
+  if (n_blocks * ncs > INT32_MAX) return aosb::set_error(err, cap, AOSB_ERR_SIZE, "too many row blocks");
+  dim3 g((unsigned)(n_blocks * ncs), np);
+  aosb::shifted_residual_blocks_kernel<<<g, aosb::kResWarps * 32, 0, (cudaStream_t)stream>>>(
       n_blocks, row_blocks, nrhs, indptr, indices, (const float2*)h_values,
       (const float2*)s_values, nnz, pencil_k, (const double2*)shifts, (const double2*)b,
       b_stride, (const double2*)x, (double2*)r, n);

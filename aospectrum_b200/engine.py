@@ -101,12 +101,17 @@ class PlanSummary:
 
 
 class BlochDevice:
-    """CSR pattern of a bundle plus device-resident block values."""
+    """CSR pattern of a bundle plus device-resident block values.
 
-    def __init__(self, bundle: LocalizedOperatorBundle, device: Any) -> None:
+    With ``upload=False`` only the host side is built (pattern, tables);
+    ``upload`` then copies the tables and block values to the device."""
+
+    def __init__(self, bundle: LocalizedOperatorBundle, device: Any, *,
+                 upload: bool = True) -> None:
         torch = _torch()
         lib = native.library()
         ops = bundle.operators
+        self.bundle = bundle
         self.n = bundle.n_orbitals
         offsets = np.ascontiguousarray(bundle.basis.atom_offsets, dtype=np.int64)
         rows = np.ascontiguousarray(ops.row_atom, dtype=np.int32)
@@ -119,8 +124,6 @@ class BlochDevice:
                         ops.n_blocks, rows.ctypes.data, cols.ctypes.data, shifts.ctypes.data,
                         boff.ctypes.data, native.C.byref(handle))
         self.handle = handle
-        with torch.cuda.device(device):
-            native.call("aosb_bloch_upload", handle)
         nnz, nsh = native.c_i64(), native.c_i64()
         lib.aosb_bloch_info(handle, native.C.byref(nnz), native.C.byref(nsh))
         self.nnz, self.n_shifts = int(nnz.value), int(nsh.value)
@@ -130,18 +133,36 @@ class BlochDevice:
         self.block_shift = np.empty(ops.n_blocks, dtype=np.int32)
         lib.aosb_bloch_export(handle, self.indptr.ctypes.data, self.indices.ctypes.data,
                               self.shifts.ctypes.data, self.block_shift.ctypes.data)
-        dptr, dind = native.c_vp(), native.c_vp()
-        lib.aosb_bloch_device_pattern(handle, native.C.byref(dptr), native.C.byref(dind))
-        self.d_indptr, self.d_indices = int(dptr.value), int(dind.value)
         complex_values = np.iscomplexobj(ops.h_values) or np.iscomplexobj(ops.s_values)
         self.value_kind = 1 if complex_values else 0
-        dtype = np.complex64 if complex_values else np.float32
+        self.device = device
+        self.uploaded = False
+        if upload:
+            self.upload()
+
+    def value_bytes(self) -> int:
+        ops = self.bundle.operators
+        item = 8 if self.value_kind else 4
+        return int((np.asarray(ops.h_values).size + np.asarray(ops.s_values).size) * item)
+
+    def upload(self) -> None:
+        if self.uploaded:
+            return
+        torch = _torch()
+        lib = native.library()
+        with torch.cuda.device(self.device):
+            native.call("aosb_bloch_upload", self.handle)
+        dptr, dind = native.c_vp(), native.c_vp()
+        lib.aosb_bloch_device_pattern(self.handle, native.C.byref(dptr), native.C.byref(dind))
+        self.d_indptr, self.d_indices = int(dptr.value), int(dind.value)
+        ops = self.bundle.operators
+        dtype = np.complex64 if self.value_kind else np.float32
         hv = np.array(ops.h_values, dtype=dtype, copy=True)
         sv = np.array(ops.s_values, dtype=dtype, copy=True)
-        tdt = torch.complex64 if complex_values else torch.float32
-        self.h_values = torch.from_numpy(hv).to(device=device, dtype=tdt)
-        self.s_values = torch.from_numpy(sv).to(device=device, dtype=tdt)
-        self.device = device
+        tdt = torch.complex64 if self.value_kind else torch.float32
+        self.h_values = torch.from_numpy(hv).to(device=self.device, dtype=tdt)
+        self.s_values = torch.from_numpy(sv).to(device=self.device, dtype=tdt)
+        self.uploaded = True
 
     def phases(self, kpoints: np.ndarray) -> np.ndarray:
         """exp(2 pi i R.k) per k and distinct shift, with the reference's
@@ -286,19 +307,75 @@ def pencil_schedule(n_k: int, shifts: np.ndarray, pair: bool) -> list[PencilWork
     return items
 
 
+class BundleResources:
+    """Device state of one bundle that several engines (requests) can share:
+    the Bloch tables with the resident block values, the CSR pattern, the
+    symbolic plan and the row blocks.  Construction is host-only (pattern,
+    analysis), so the footprint is known before any device memory is
+    taken; ``upload`` moves everything to the device."""
+
+    def __init__(self, bundle: LocalizedOperatorBundle, device: Any, *, tile: int,
+                 ordering: str = "auto") -> None:
+        torch = _torch()
+        self.device = torch.device(device)
+        self.bundle = bundle
+        self.bloch = BlochDevice(bundle, self.device, upload=False)
+        supervariables = np.asarray(bundle.basis.atom_offsets)
+        self.plan = SymbolicPlan(self.bloch.n, self.bloch.indptr, self.bloch.indices, tile=tile,
+                                 supervariables=supervariables, ordering=ordering,
+                                 device=self.device, upload=False)
+        self._rb = row_blocks(self.bloch.indptr, self.bloch.indices, starts=supervariables[:-1])
+        self.row_blocks = None
+        self.uploaded = False
+
+    def upload(self) -> None:
+        if self.uploaded:
+            return
+        torch = _torch()
+        self.bloch.upload()
+        self.plan.upload()
+        self.row_blocks = torch.from_numpy(self._rb).to(self.device)
+        self.uploaded = True
+
+    def resident_bytes(self) -> int:
+        """Device bytes held while the bundle stays resident."""
+        b = self.bloch
+        pattern = 8 * (b.n + 1) + 4 * b.nnz
+        info = self.plan.info
+        plan = 4 * (3 * info.n_pad + 4 * info.n_tiles * info.n_tiles) + 4 * info.n_slots
+        return int(b.value_bytes() + 2 * pattern + plan + 4 * self._rb.size)
+
+    def close(self) -> None:
+        self.bloch.close()
+        self.plan.close()
+
+
 class BandEngine:
     """Device-resident Band solver for one bundle."""
 
     def __init__(self, bundle: LocalizedOperatorBundle | None,
                  settings: CissSettings | None = None, engine: EngineSettings | None = None,
-                 device: Any = None, *, csr: tuple[int, np.ndarray, np.ndarray] | None = None
-                 ) -> None:
+                 device: Any = None, *, csr: tuple[int, np.ndarray, np.ndarray] | None = None,
+                 resources: BundleResources | None = None) -> None:
         torch = _torch()
         self.bundle = bundle
         self.settings = settings or CissSettings()
         self.engine = engine or EngineSettings()
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None
                                    else torch.device(device).index or 0)
+        self._owns = resources is None
+        if resources is not None:
+            resources.upload()
+            self.bundle = resources.bundle
+            self.n = resources.bloch.n
+            self.bloch = self.pattern = resources.bloch
+            self.plan = resources.plan
+            self.row_blocks = resources.row_blocks
+            self.pattern_seconds = self.analysis_seconds = 0.0
+            if self.settings.search_dimension >= self.n:
+                raise SolverError("CISS search dimension must be smaller than matrix dimension")
+            self._init_buffers()
+            return
         t0 = perf_counter()
         if bundle is not None:
             self.n = bundle.n_orbitals
@@ -325,6 +402,10 @@ class BandEngine:
                                  supervariables=supervariables, ordering=self.engine.ordering,
                                  device=self.device)
         self.analysis_seconds = perf_counter() - t0
+        self._init_buffers()
+
+    def _init_buffers(self) -> None:
+        torch = _torch()
         q = probe_block(self.n, self.settings)
         self.probes = torch.from_numpy(q.astype(np.complex128)).to(self.device)
         self._gram_scratch = None
@@ -407,7 +488,7 @@ class BandEngine:
         if len(kp) != 3:
             raise InputError("k point must contain three values")
         h, s = self.bloch.apply(np.asarray([kp]))
-        torch.cuda.synchronize(self.device)
+        torch.cuda.current_stream(self.device).synchronize()
         hv, sv = h[0].cpu().numpy(), s[0].cpu().numpy()
         ip = self.bloch.indptr
         ix = self.bloch.indices
@@ -448,7 +529,7 @@ class BandEngine:
         torch.cuda.reset_peak_memory_stats(dev)
         t0 = perf_counter()
         hvals, svals = self.bloch.apply(kp)
-        torch.cuda.synchronize(dev)
+        torch.cuda.current_stream(dev).synchronize()
         assembly = perf_counter() - t0
         results = self._ciss(hvals, svals, interval, {"bloch_assembly": assembly}, t0)
         return results, [assembly / kp.shape[0]] * kp.shape[0]
@@ -464,7 +545,7 @@ class BandEngine:
         dev = self.device
 
         def tick(name: str, t0: float) -> float:
-            torch.cuda.synchronize(dev)
+            torch.cuda.current_stream(dev).synchronize()
             t1 = perf_counter()
             stages[name] = stages.get(name, 0.0) + (t1 - t0)
             return t1
@@ -482,8 +563,11 @@ class BandEngine:
         cap = min(self.max_pencils(L), len(work))
         info = self.plan.info
         lib = native.library()
-        precision = (native.PRECISION_BF16X3 if mixed and self.engine.tensor_cores
-                     else native.PRECISION_PLAIN)
+        if mixed and self.engine.tensor_cores:
+            precision = (native.PRECISION_BF16X3 if self.engine.tensor_core_panels
+                         else native.PRECISION_BF16X3_FP32_PANELS)
+        else:
+            precision = native.PRECISION_PLAIN
         fbytes = lib.aosb_factor_bytes(self.plan.handle, cap)
         factor = torch.empty(fbytes // 4, dtype=torch.float32, device=dev)
         pivots = torch.empty((cap, info.n_pad), dtype=torch.int32, device=dev)
@@ -582,7 +666,7 @@ class BandEngine:
             if it < steps:
                 self._residual(n, L, np_, hvals, svals, pk, z, b, xn, rr, st)
 
-    residual_kernel = "rows"   # "rows" or "blocks" (row blocks of one atom)
+    residual_kernel = "blocks"   # "blocks" (rows of one atom share x loads) or "rows"
 
     def _residual(self, n, L, np_, hvals, svals, pk, z, b, xn, rr, st) -> None:
         """FP64 r = b - (H - z S) x for every pencil of the batch."""
@@ -612,7 +696,7 @@ class BandEngine:
         transform, sigma = truncate_gram(gram, st.rank_relative_tolerance)
         basis = self._dense_mul(mom, torch.from_numpy(transform).to(dev))
         saturated = basis.shape[1] == st.search_dimension
-        torch.cuda.synchronize(dev)
+        torch.cuda.current_stream(dev).synchronize()
         local["subspace_compression"] = perf_counter() - t
         t = perf_counter()
         hb = torch.empty_like(basis)
@@ -646,5 +730,6 @@ class BandEngine:
                           not saturated)
 
     def close(self) -> None:
-        self.pattern.close()
-        self.plan.close()
+        if self._owns:
+            self.pattern.close()
+            self.plan.close()

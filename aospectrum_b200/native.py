@@ -23,6 +23,7 @@ ERROR_CAPACITY = 512
 
 PRECISION_PLAIN = 0
 PRECISION_BF16X3 = 1
+PRECISION_BF16X3_FP32_PANELS = 2
 
 STATUS_NAMES = {
     10: "ABI mismatch", 11: "dimensions", 12: "batch", 13: "null pointer",
@@ -92,6 +93,9 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_abi_version": (c_u32, []),
     "aosb_build_info": (C.c_char_p, []),
     "aosb_launch_count": (C.c_uint64, []),
+    "aosb_kernel_timing": (C.c_int, [c_i32]),
+    "aosb_kernel_timing_read": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), C.POINTER(c_i64)]),
     "aospectrum_b200_solve_complex64_ubatch_v1": (C.c_int, [C.POINTER(UbatchRequest),
                                                             C.POINTER(UbatchResult)]),
     "aosb_bloch_create": (C.c_int, [c_i64, c_i64, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp,

@@ -242,6 +242,7 @@ def main() -> None:
     launches0 = native.library().aosb_launch_count()
     eng.profile_factor = True
     eng.factor_times_ms = []
+    native.library().aosb_kernel_timing(1)
     barrier()
     torch.cuda.synchronize(dev)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -257,6 +258,11 @@ def main() -> None:
     elapsed = start.elapsed_time(stop) / 1e3
     launches = native.library().aosb_launch_count() - launches0
     eng.profile_factor = False
+    k_ms, k_flops, k_bytes, k_launches = (native.C.c_double(), native.C.c_double(),
+                                          native.C.c_double(), native.c_i64())
+    native.library().aosb_kernel_timing_read(native.C.byref(k_ms), native.C.byref(k_flops),
+                                             native.C.byref(k_bytes), native.C.byref(k_launches))
+    native.library().aosb_kernel_timing(0)
     t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -265,29 +271,44 @@ def main() -> None:
     value = total_k / elapsed
     stats = dict(eng.last_stats)
     info = eng.plan.info
-    # roofline of the factorization (the dominant kernel group)
-    ft = eng.factor_times_ms
-    per_pencil_flops = info.factor_flops_alg
+    # roofline of the dominant kernel: the tensor-core Schur update
+    # (schur_tc_kernel), timed with CUDA events on its launch stream over the
+    # timed region; algorithmic flops = 8 T^3 per (target tile, pencil).
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (
         ROOT / "MEASURED_PEAKS.json").exists() else {}
     tc = args.precision == "mixed" and bool(args.tensor_cores)
-    if tc:
-        peak = peaks.get("bf16_tflops_sustained", 1400.0) / 3.0
-        peak_note = "measured sustained bf16 / 3 (split-BF16 needs 3 products)"
+    ft = eng.factor_times_ms
+    factor_tflops = (info.factor_flops_alg * float(np.mean(eng.factor_pencils)) /
+                     (float(np.mean(ft)) / 1e3) / 1e12) if ft else None
+    if tc and k_launches.value > 0:
+        sustained = peaks.get("bf16_tflops_sustained")
+        peak = (sustained if sustained else 1400.0) / 3.0
+        achieved = k_flops.value / (k_ms.value / 1e3) / 1e12
+        per_launch_targets = k_flops.value / k_launches.value / (8.0 * info.tile ** 3)
+        traffic = schur_traffic_per_target()
+        roofline = {
+            "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak,
+            "traffic": traffic * per_launch_targets if traffic else None,
+            "kernel": "schur_tc_kernel",
+            "launches": int(k_launches.value),
+            "avg_launch_ms": k_ms.value / k_launches.value,
+            "algorithmic_flops_per_launch": k_flops.value / k_launches.value,
+            "algorithmic_bytes_per_launch": k_bytes.value / k_launches.value,
+            "achieved_hbm_gbs": k_bytes.value / (k_ms.value / 1e3) / 1e9,
+            "hbm_peak_gbs": peaks.get("hbm_gbs", 6650.0),
+            "peak_source": ("of measured: MEASURED_PEAKS.json bf16_tflops_sustained / 3 "
+                            "(split BF16 issues 3 products per algorithmic product)"
+                            if sustained else "of fallback: 1400 TFLOP/s sustained / 3"),
+            "factorization_tflops": factor_tflops,
+            "flops_per_factorization": info.factor_flops_alg}
     else:
         peak = 74.4
-        peak_note = "nominal FP32 SIMT 148 SM x 128 lanes x 2 x 1.965 GHz (no measured FP32 peak)"
-    if ft:
-        pencils = stats.get("pencil_batch", 1)
-        achieved = per_pencil_flops * np.mean([p for p in eng.factor_pencils]) / (
-            np.mean(ft) / 1e3) / 1e12
-    else:
-        achieved = None
-    roofline = {"bound": "tensor" if tc else "fp32-simt", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
-                "traffic": None, "kernel": "tile LU factorization (schur-dominated)",
-                "peak_source": peak_note,
-                "flops_per_factorization": per_pencil_flops}
+        roofline = {"bound": "fp32-simt", "achieved": factor_tflops, "peak": peak,
+                    "unit": "TFLOP/s", "frac": (factor_tflops / peak) if factor_tflops else None,
+                    "traffic": None, "kernel": "tile LU factorization (FP32 SIMT)",
+                    "peak_source": "nominal FP32 SIMT 148 SM x 128 lanes x 2 x 1.965 GHz",
+                    "flops_per_factorization": info.factor_flops_alg}
     out = {
         "metric": "k-points/s at <=1e-4 eV vs FP64 (mixed+batched CISS, 1 B200)",
         "value": value, "unit": "k-points/s", "n_gpus": world, "steps": args.steps,
@@ -359,6 +380,16 @@ def main() -> None:
     eng.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def schur_traffic_per_target() -> float | None:
+    """DRAM bytes per (target tile, pencil) of schur_tc_kernel from the
+    committed ncu capture summary (dram__bytes_read.sum + write.sum of one
+    launch divided by the targets it updated)."""
+    f = ROOT / "profiles" / "schur_tc_kernel_c2.json"
+    if not f.exists():
+        return None
+    return float(json.loads(f.read_text())["dram_bytes_per_target"])
 
 
 def fp64_window(pair, interval, dev) -> np.ndarray:

@@ -79,6 +79,17 @@ const char *aosb_build_info(void);
 /* Kernels launched by this library since load (all devices and threads). */
 uint64_t aosb_launch_count(void);
 
+/* Measurement hook (no counterpart in the reference, whose cuDSS calls are
+ * opaque): aosb_kernel_timing(1) clears and starts CUDA-event timing of
+ * every tensor-core Schur-update launch (schur_tc_kernel) on the stream it
+ * is launched on; aosb_kernel_timing(0) stops.  _read synchronizes on the
+ * recorded events and returns the summed device time (ms), the algorithmic
+ * flops (8 T^3 per target tile and pencil), the algorithmic bytes (target
+ * read + write, staged operands read once) and the number of launches. */
+int aosb_kernel_timing(int32_t enable);
+int aosb_kernel_timing_read(double *total_ms, double *flops, double *bytes,
+                            int64_t *launches);
+
 /* ------------------------------------------------------------------------
  * Drop-in uniform-batch shifted solve with host buffers.
  * Replaces aospectrum_cudss_solve_complex64_ubatch_v1
@@ -236,7 +247,10 @@ void aosb_plan_destroy(aosb_plan_t *plan);
  * diagonal.
  * ------------------------------------------------------------------------ */
 #define AOSB_PRECISION_PLAIN 0  /* complex64, FP32 SIMT updates */
-#define AOSB_PRECISION_BF16X3 1 /* split-BF16 tcgen05 updates, FP32 accumulate */
+#define AOSB_PRECISION_BF16X3 1 /* split-BF16 tcgen05 panels and Schur updates,
+                                   FP32 accumulate (tile 128) */
+#define AOSB_PRECISION_BF16X3_FP32_PANELS 2 /* split-BF16 tcgen05 Schur updates,
+                                               FP32 SIMT panels (tile 128) */
 
 typedef struct {
   uint32_t abi_version;

@@ -169,9 +169,11 @@ def test_plain_factor_solve_matches_superlu(case, tile, ordering, torch):
         plan.close()
 
 
+@pytest.mark.parametrize("precision", [1, 2])
 @pytest.mark.parametrize("case", ["small2d", "c1"])
-def test_tensor_core_factor_matches_superlu(case, torch):
-    """Split-BF16 tcgen05 Schur updates: unrefined solves within 1e-3, FP64
+def test_tensor_core_factor_matches_superlu(case, precision, torch):
+    """Split-BF16 tcgen05 Schur updates (precision 1: tensor-core panels
+    too; 2: FP32 SIMT panels): unrefined solves within 1e-3, FP64
     refinement to 1e-9, both directions."""
     b = getattr(bundles, case)()
     dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[1], torch, 128)
@@ -179,10 +181,10 @@ def test_tensor_core_factor_matches_superlu(case, torch):
         rng = np.random.default_rng(3)
         rhs = (rng.standard_normal((dev.n, 8)) + 1j * rng.standard_normal((dev.n, 8)))
         shifts = [-2.6 + 0.004j, -2.4 + 0.04j, -1.0 + 0.5j]
-        x0 = _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=1)
+        x0 = _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=precision)
         for adjoint in (0, 1):
-            x = _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=1, adjoint=adjoint,
-                              steps=3)
+            x = _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=precision,
+                              adjoint=adjoint, steps=3)
             for p, z in enumerate(shifts):
                 ref = _splu_reference(dev, h, s, z, rhs, adjoint=bool(adjoint))
                 if adjoint == 0:
