@@ -91,6 +91,9 @@ class EngineSettings:
     tensor_core_panels: with tensor cores, also form the panel tiles
         L_ik = A_ik inv(U_kk) and U_kj = inv(L_kk) P_k A_kj in split BF16;
         False keeps them in FP32 SIMT.
+    tensor_core_solves: with tensor cores, run the off-diagonal tile
+        updates of the triangular sweeps in split BF16 too (FP64
+        refinement recovers the accuracy); False keeps them in FP32 SIMT.
     """
 
     precision: str = "mixed"
@@ -101,6 +104,7 @@ class EngineSettings:
     ordering: str = "auto"
     tensor_cores: bool = True
     tensor_core_panels: bool = True
+    tensor_core_solves: bool = False
 
     def __post_init__(self) -> None:
         if self.precision not in PRECISIONS:

@@ -567,11 +567,11 @@ int factor_step_panels(const aosb_plan* P, const aosb_factor_args_v1* a, int k, 
   return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "unsupported tile size");
 }
 
-int factor_step_diag(const aosb_plan* P, const aosb_factor_args_v1* a, int k, char* err,
-                     size_t cap) {
+int factor_step_diag(const aosb_plan* P, const aosb_factor_args_v1* a, int k, cudaStream_t st,
+                     char* err, size_t cap) {
   if (P->T != 128) return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "diagonal step needs tile 128");
   if (int rc = ensure_diag_attr<128>(err, cap)) return rc;
-  diag_lu_kernel<128><<<a->n_pencils, kDiagThreads, diag_smem_bytes<128>(), (cudaStream_t)a->stream>>>(
+  diag_lu_kernel<128><<<a->n_pencils, kDiagThreads, diag_smem_bytes<128>(), st>>>(
       k, P->d_diag_slot, P->n_slots, P->n_pad, a->factor, a->pivots, a->status);
   count_launches(1);
   return 0;

@@ -1,8 +1,11 @@
-// Tensor-core (tcgen05) factorization path: split-BF16 Schur updates.
+// Tensor-core (tcgen05) factorization path: split-BF16 panel products and
+// Schur updates.
 //
-// Same right-looking tile LU as factor.cu (diagonal LU and panels stay FP32
-// SIMT); the Schur update A_ij -= L_ik U_kj of every step runs on the 5th
-// generation tensor cores:
+// Same right-looking tile LU as factor.cu.  The diagonal tile LU (with
+// pivoting and the two triangle inverses) stays FP32 SIMT; the panel
+// products L_ik = A_ik inv(U_kk), U_kj = inv(L_kk) P_k A_kj and the Schur
+// update A_ij -= L_ik U_kj of every step run on the 5th generation tensor
+// cores:
 //
 //   * stage_kernel converts the step's L tiles (i,k) and U tiles (k,j) into
 //     four BF16 planes each -- re_hi, re_lo, im_hi, im_lo with
@@ -26,11 +29,13 @@
 #include "plan.h"
 #include "factor.h"
 #include "cgemm.cuh"
+#include "tc_common.cuh"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -54,13 +59,14 @@ SchurTimer& schur_timer() {
 
 namespace {
 
+using namespace tc;
+
 constexpr int kTcT = 128;                 // tile edge supported by this path
 constexpr int kSlabK = 16;                // K per slab (one MMA K step)
 constexpr int kSlabs = kTcT / kSlabK;     // 8
 constexpr int kPlaneSlabBytes = kTcT * kSlabK * 2;          // 4096
 constexpr int kOperandSlabBytes = 4 * kPlaneSlabBytes;      // 16384
 constexpr int kStagedTileBytes = kSlabs * kOperandSlabBytes;  // 131072
-constexpr long long kWaitLimit = 1ll << 22;  // polls (with backoff) before timeout
 
 __device__ __forceinline__ size_t tile_base(int64_t p, int64_t n_slots, int64_t slot) {
   return ((size_t)p * (size_t)n_slots + (size_t)slot) * (size_t)(2 * kTcT * kTcT);
@@ -176,123 +182,6 @@ __global__ void __launch_bounds__(256) stage_kernel(int nL, int nU, int panel, i
   stage_tile(F, out, kind, pv);
 }
 
-// ---------------------------------------------------------------------------
-// PTX helpers.
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-// Bounded wait on phase `parity`; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t addr = smem_u32(bar);
-  for (long long it = 0; it < kWaitLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (it > 64) __nanosleep(128);
-  }
-  return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-
-// UMMA shared-memory descriptor: K-major, no swizzle.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version (Blackwell)
-  return d;               // base offset 0, lbo mode 0, layout SWIZZLE_NONE (0)
-}
-
-// Instruction descriptor: BF16 x BF16 -> F32, K-major A and B, M = N = 128.
-__host__ __device__ constexpr uint32_t umma_idesc(bool negate_a) {
-  return (1u << 4)                    // D format F32
-         | (1u << 7)                  // A format BF16
-         | (1u << 10)                 // B format BF16
-         | ((negate_a ? 1u : 0u) << 13)
-         | ((uint32_t)(kTcT >> 3) << 17)   // N / 8
-         | ((uint32_t)(kTcT >> 4) << 24);  // M / 16
-}
-
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
-                                          uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   smem_u32(bar))
-               : "memory");
-}
-
-// C[box at (x, y)] += smem tile (FP32 add in L2), one bulk group per commit.
-__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, const void* src, int x,
-                                                  int y) {
-  asm volatile(
-      "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
-          reinterpret_cast<uint64_t>(map)),
-      "r"(smem_u32(src)), "r"(x), "r"(y)
-      : "memory");
-}
-// C[box at (x, y)] = smem tile.
-__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y) {
-  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
-                   reinterpret_cast<uint64_t>(map)),
-               "r"(smem_u32(src)), "r"(x), "r"(y)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_all() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
 // Persistent, warp-specialized Schur update.  Each CTA (one per SM) walks
 // the step's (pencil, target) items with stride gridDim.x:
 //   warp 8 lane 0  producer: 16-wide K slabs of A (L_ik) and B (U_kj) into a
@@ -325,39 +214,68 @@ struct PShared {
   alignas(1024) float ep[kEpiWarps][2][32 * 32];
 };
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 // Work item -> (staged A index, staged B index, target slot).
-//   Schur (panel == 0): pair = a * nU + b over the step's L x U tiles; the
-//     target gets C -= A B (TMA reduce-add of -acc).
-//   Panel (panel == 1): pair < nL: L_ik = A_ik inv(U_kk); else
-//     U_kj = inv(L_kk) P_k A_kj; the target is overwritten with A B (TMA
-//     store of acc).
+//   kMapSchur: pair = a * nU + b over the step's L x U tiles; the target
+//     gets C -= A B (TMA reduce-add of -acc).
+//   kMapPanel: pair < nL: L_ik = A_ik inv(U_kk); else U_kj = inv(L_kk) P_k
+//     A_kj; the target is overwritten with A B (TMA store of acc).
+//   kMapCross / kMapRest: the Schur pairs split for lookahead.  With a0
+//     (b0) = 1 when the step's first L (U) tile is in tile row (column)
+//     k + 1, "cross" holds the pairs with a < a0 or b < b0 -- every target
+//     in tile row or column k + 1, which step k + 1's diagonal LU and panels
+//     read -- and "rest" the pairs with a >= a0 and b >= b0.
+enum MapKind : int { kMapSchur = 0, kMapPanel = 1, kMapCross = 2, kMapRest = 3 };
+
 struct ItemMap {
-  int panel, nL, nU, n_pairs;
+  int kind, nL, nU, n_pairs, a0, b0;
   const int32_t* tslot;  // Schur targets [nL * nU]
   const int32_t* lslot;  // panel L targets [nL]
   const int32_t* uslot;  // panel U targets [nU]
 };
 
-__device__ __forceinline__ void item_operands(const ItemMap& m, int pair, int& ia, int& ib) {
-  if (!m.panel) {
-    ia = pair / m.nU;
-    ib = m.nL + pair % m.nU;
-  } else if (pair < m.nL) {
-    ia = pair;
-    ib = m.nL + m.nU + 1;
-  } else {
-    ia = m.nL + m.nU;
-    ib = pair;
+__device__ __forceinline__ void item_pair(const ItemMap& m, int pair, int& a, int& b) {
+  if (m.kind == kMapSchur) {
+    a = pair / m.nU;
+    b = pair % m.nU;
+  } else if (m.kind == kMapRest) {
+    const int w = m.nU - m.b0;
+    a = m.a0 + pair / w;
+    b = m.b0 + pair % w;
+  } else {  // kMapCross
+    const int head = m.a0 * m.nU;
+    if (pair < head) {
+      a = pair / m.nU;
+      b = pair % m.nU;
+    } else {
+      const int i = pair - head;
+      a = m.a0 + i / m.b0;
+      b = i % m.b0;
+    }
   }
 }
 
+__device__ __forceinline__ void item_operands(const ItemMap& m, int pair, int& ia, int& ib) {
+  if (m.kind == kMapPanel) {
+    if (pair < m.nL) {
+      ia = pair;
+      ib = m.nL + m.nU + 1;
+    } else {
+      ia = m.nL + m.nU;
+      ib = pair;
+    }
+    return;
+  }
+  int a, b;
+  item_pair(m, pair, a, b);
+  ia = a;
+  ib = m.nL + b;
+}
+
 __device__ __forceinline__ int item_target(const ItemMap& m, int pair) {
-  if (!m.panel) return m.tslot[pair];
-  return pair < m.nL ? m.lslot[pair] : m.uslot[pair - m.nL];
+  if (m.kind == kMapPanel) return pair < m.nL ? m.lslot[pair] : m.uslot[pair - m.nL];
+  int a, b;
+  item_pair(m, pair, a, b);
+  return m.tslot[a * m.nU + b];
 }
 
 __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
@@ -422,7 +340,7 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     }
   } else if (warp == kEpiWarps + 1) {
     if (lane == 0) {
-      const uint32_t id_pos = umma_idesc(false), id_neg = umma_idesc(true);
+      const uint32_t id_pos = umma_idesc_mn(kTcT, kTcT, false), id_neg = umma_idesc_mn(kTcT, kTcT, true);
       const uint32_t lbo = (kTcT / 8) * 128, sbo = 128;
       int stage = 0, acc = 0;
       uint32_t phase = 0, acc_phase = 0;
@@ -486,7 +404,8 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     float* bre = sh.ep[warp][0];
     float* bim = sh.ep[warp][1];
     const int sw = lane & 7;
-    const float sgn = map.panel ? 1.0f : -1.0f;  // store acc / add -acc
+    const bool store = map.kind == kMapPanel;
+    const float sgn = store ? 1.0f : -1.0f;  // store acc / add -acc
     int acc = 0;
     uint32_t acc_phase = 0;
     for (int it = blockIdx.x; it < total; it += gridDim.x) {
@@ -532,7 +451,7 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
         if (lane == 0) {
           const int x = half * 64 + bk * 32;
           const int y = (int)(row0 + quarter * 32);
-          if (map.panel) {
+          if (store) {
             tma_store_2d(&tmap_c, bre, x, y);
             tma_store_2d(&tmap_c, bim, x, y + kTcT);
           } else {
@@ -568,9 +487,35 @@ static int64_t staged_tiles_per_pencil(const aosb_plan* P) {
   return most + 2;
 }
 
+// Two staging buffers: with lookahead, step k + 1's panels are staged while
+// step k's Schur update still reads step k's tiles.
 size_t factor_tc_workspace(const aosb_plan* P, int32_t n_pencils) {
   if (P->T != kTcT) return 0;
-  return (size_t)staged_tiles_per_pencil(P) * kStagedTileBytes * (size_t)n_pencils;
+  return 2 * (size_t)staged_tiles_per_pencil(P) * kStagedTileBytes * (size_t)n_pencils;
+}
+
+// Side stream of a caller stream for the lookahead panels (created once,
+// non-blocking, kept for the life of the process).
+static int side_stream(cudaStream_t main, cudaStream_t* out, char* err, size_t cap) {
+  static std::mutex mu;
+  static std::vector<std::pair<cudaStream_t, cudaStream_t>> table;
+  int device = 0;
+  cudaGetDevice(&device);
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto& e : table) {
+    if (e.first == main) {
+      int dev2 = -1;
+      if (cudaStreamGetDevice(e.second, &dev2) == cudaSuccess && dev2 == device) {
+        *out = e.second;
+        return 0;
+      }
+    }
+  }
+  cudaStream_t s = nullptr;
+  AOSB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), err, cap);
+  table.emplace_back(main, s);
+  *out = s;
+  return 0;
 }
 
 // Tensor map of the factor storage as a [rows][T] FP32 matrix (each tile is
@@ -634,35 +579,69 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   if (int rc = factor_tensor_map(a->factor, (int64_t)np * P->n_slots * 2 * kTcT, &tmap_c, err, cap))
     return rc;
   const bool tc_panels = a->precision != AOSB_PRECISION_BF16X3_FP32_PANELS;
-  auto grid_for = [&](int64_t items) { return (int)(items < sms ? items : sms); };
-  for (int64_t k = 0; k < P->nb; ++k) {
+  auto grid_for = [&](int64_t items, int cap_ctas) {
+    return (int)(items < cap_ctas ? items : cap_ctas);
+  };
+  // Lookahead (tensor-core panels): step k's Schur targets in tile row and
+  // column k + 1 go first ("cross"); then step k + 1's diagonal LU, panel
+  // products and staging run on a side stream on `reserve` SMs while the
+  // rest of step k's Schur update runs on the others.
+  const bool lookahead = tc_panels && sms >= 32;
+  const int reserve = lookahead ? std::min(std::max(np, 8), sms / 4) : 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_cross = nullptr, ev_panel = nullptr;
+  if (lookahead) {
+    if (int rc = side_stream(st, &side, err, cap)) return rc;
+    AOSB_CUDA_TRY(cudaEventCreateWithFlags(&ev_cross, cudaEventDisableTiming), err, cap);
+    if (cudaEventCreateWithFlags(&ev_panel, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventDestroy(ev_cross);
+      return set_error(err, cap, AOSB_ERR_CUDA, "cudaEventCreate failed");
+    }
+  }
+  struct EventGuard {
+    cudaEvent_t a, b;
+    ~EventGuard() {
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } guard{ev_cross, ev_panel};
+  const int64_t buffer_bytes = (int64_t)np * pencil_stride;
+  auto stage_buf = [&](int64_t k) { return staging + (k & 1) * buffer_bytes; };
+
+  // diagonal LU + panel products of step k on stream s (panel grid <= cap_ctas)
+  auto panels = [&](int64_t k, cudaStream_t s, int cap_ctas) -> int {
+    if (int rc = factor_step_diag(P, a, (int)k, s, err, cap)) return rc;
     const int nL = P->lb_off[k + 1] - P->lb_off[k];
     const int nU = P->ur_off[k + 1] - P->ur_off[k];
+    if (nL + nU == 0) return 0;
     const int32_t* lslot = P->d_lb_slot + P->lb_off[k];
     const int32_t* uslot = P->d_ur_slot + P->ur_off[k];
-    if (!tc_panels) {
-      if (int rc = factor_step_panels(P, a, (int)k, err, cap)) return rc;
-    } else {
-      if (int rc = factor_step_diag(P, a, (int)k, err, cap)) return rc;
-      if (nL + nU > 0) {
-        // L_ik = A_ik inv(U_kk), U_kj = inv(L_kk) P_k A_kj on the tensor cores
-        stage_kernel<<<dim3(nL + nU + 2, np), 256, 0, st>>>(
-            nL, nU, 1, (int)k, lslot, uslot, P->diag_slot[k], P->n_slots, P->n_pad, a->factor,
-            a->pivots, staging, pencil_stride);
-        const ItemMap pm{1, nL, nU, nL + nU, nullptr, lslot, uslot};
-        schur_tc_kernel<<<grid_for((int64_t)(nL + nU) * np), kPThreads, smem, st>>>(
-            pm, np, P->n_slots, staging, pencil_stride, a->status, tmap_c);
-        count_launches(2);
-      }
-    }
-    if (nL == 0 || nU == 0) continue;
-    stage_kernel<<<dim3(nL + nU, np), 256, 0, st>>>(nL, nU, 0, (int)k, lslot, uslot, 0, P->n_slots,
-                                                   P->n_pad, a->factor, a->pivots, staging,
-                                                   pencil_stride);
-    const int64_t items = (int64_t)nL * nU * np;
-    if ((int64_t)nL * nU > INT32_MAX / 65536)
-      return set_error(err, cap, AOSB_ERR_SIZE, "too many Schur targets in one step");
-    const int grid = grid_for(items);
+    // L_ik = A_ik inv(U_kk), U_kj = inv(L_kk) P_k A_kj on the tensor cores
+    stage_kernel<<<dim3(nL + nU + 2, np), 256, 0, s>>>(
+        nL, nU, 1, (int)k, lslot, uslot, P->diag_slot[k], P->n_slots, P->n_pad, a->factor,
+        a->pivots, stage_buf(k), pencil_stride);
+    const ItemMap pm{kMapPanel, nL, nU, nL + nU, 0, 0, nullptr, lslot, uslot};
+    schur_tc_kernel<<<grid_for((int64_t)(nL + nU) * np, cap_ctas), kPThreads, smem, s>>>(
+        pm, np, P->n_slots, stage_buf(k), pencil_stride, a->status, tmap_c);
+    count_launches(2);
+    return 0;
+  };
+  // Schur staging of step k (L_ik as A, U_kj as B) on stream s
+  auto stage_schur = [&](int64_t k, cudaStream_t s) {
+    const int nL = P->lb_off[k + 1] - P->lb_off[k];
+    const int nU = P->ur_off[k + 1] - P->ur_off[k];
+    if (nL == 0 || nU == 0) return;
+    stage_kernel<<<dim3(nL + nU, np), 256, 0, s>>>(nL, nU, 0, (int)k, P->d_lb_slot + P->lb_off[k],
+                                                  P->d_ur_slot + P->ur_off[k], 0, P->n_slots,
+                                                  P->n_pad, a->factor, a->pivots, stage_buf(k),
+                                                  pencil_stride);
+    count_launches(1);
+  };
+  // Schur update of step k (the pairs `kind` selects) on the caller stream
+  auto schur = [&](int64_t k, int kind, int a0, int b0, int n_pairs, int cap_ctas) {
+    const int nL = P->lb_off[k + 1] - P->lb_off[k];
+    const int nU = P->ur_off[k + 1] - P->ur_off[k];
+    const int64_t items = (int64_t)n_pairs * np;
     SchurTimer& tm = schur_timer();
     cudaEvent_t ev[2] = {nullptr, nullptr};
     {
@@ -674,10 +653,10 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
         ev[0] = ev[1] = nullptr;
       }
     }
-    const ItemMap sm{0, nL, nU, nL * nU, P->d_sc_slot + P->sc_off[k], nullptr, nullptr};
-    schur_tc_kernel<<<grid, kPThreads, smem, st>>>(sm, np, P->n_slots, staging, pencil_stride,
-                                                   a->status, tmap_c);
-    count_launches(2);
+    const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr};
+    schur_tc_kernel<<<grid_for(items, cap_ctas), kPThreads, smem, st>>>(
+        sm, np, P->n_slots, stage_buf(k), pencil_stride, a->status, tmap_c);
+    count_launches(1);
     if (ev[0] != nullptr) {
       cudaEventRecord(ev[1], st);
       std::lock_guard<std::mutex> lock(tm.mu);
@@ -685,9 +664,54 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
       tm.events.push_back(ev[1]);
       tm.flops += (double)items * 8.0 * kTcT * kTcT * kTcT;
       tm.bytes += (double)items * 2.0 * 2 * kTcT * kTcT * sizeof(float) +
-                  (double)(nL + nU) * np * kStagedTileBytes;
+                  (double)(nL + nU) * np * kStagedTileBytes * ((double)n_pairs / (nL * nU));
       tm.launches += 1;
     }
+  };
+
+  for (int64_t k = 0; k < P->nb; ++k) {
+    const int nL = P->lb_off[k + 1] - P->lb_off[k];
+    const int nU = P->ur_off[k + 1] - P->ur_off[k];
+    if ((int64_t)nL * nU > INT32_MAX / 65536)
+      return set_error(err, cap, AOSB_ERR_SIZE, "too many Schur targets in one step");
+    if (!tc_panels) {
+      if (int rc = factor_step_panels(P, a, (int)k, err, cap)) return rc;
+      stage_schur(k, st);
+      if (nL > 0 && nU > 0) schur(k, kMapSchur, 0, 0, nL * nU, sms);
+      continue;
+    }
+    if (k == 0) {
+      if (int rc = panels(0, st, sms)) return rc;
+      stage_schur(0, st);
+    }
+    const bool has_next = k + 1 < P->nb;
+    if (nL == 0 || nU == 0) {
+      if (has_next) {
+        if (int rc = panels(k + 1, st, sms)) return rc;
+        stage_schur(k + 1, st);
+      }
+      continue;
+    }
+    if (!lookahead || !has_next) {
+      schur(k, kMapSchur, 0, 0, nL * nU, sms);
+      if (has_next) {
+        if (int rc = panels(k + 1, st, sms)) return rc;
+        stage_schur(k + 1, st);
+      }
+      continue;
+    }
+    const int a0 = P->lb_tile[P->lb_off[k]] == k + 1 ? 1 : 0;
+    const int b0 = P->ur_tile[P->ur_off[k]] == k + 1 ? 1 : 0;
+    const int rest = (nL - a0) * (nU - b0);
+    const int cross = nL * nU - rest;
+    if (cross > 0) schur(k, kMapCross, a0, b0, cross, sms);
+    AOSB_CUDA_TRY(cudaEventRecord(ev_cross, st), err, cap);
+    AOSB_CUDA_TRY(cudaStreamWaitEvent(side, ev_cross, 0), err, cap);
+    if (int rc = panels(k + 1, side, reserve)) return rc;
+    stage_schur(k + 1, side);
+    AOSB_CUDA_TRY(cudaEventRecord(ev_panel, side), err, cap);
+    if (rest > 0) schur(k, kMapRest, a0, b0, rest, sms - reserve);
+    AOSB_CUDA_TRY(cudaStreamWaitEvent(st, ev_panel, 0), err, cap);
   }
   return launch_check(err, cap, "tensor-core factorization");
 }

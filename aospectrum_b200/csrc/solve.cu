@@ -16,6 +16,9 @@
 #include "cgemm.cuh"
 
 namespace aosb {
+int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, int op, int np,
+                    int nrhs, const aosb_plan* P, const float* factor, float2* work,
+                    const float2* ytmp, int32_t* status, cudaStream_t st, char* err, size_t cap);
 namespace {
 
 constexpr int kThreads = 256;
@@ -173,9 +176,19 @@ int run_solve(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t
       default: solve_diag_kernel<T, kLinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y); break;
     }
   };
+  const bool tc = T == 128 && (a->flags & AOSB_SOLVE_TENSOR_CORES) != 0;
+  int32_t* tc_status = (int32_t*)((unsigned char*)a->scratch + (size_t)np * T * L * sizeof(float2));
+  if (tc) AOSB_CUDA_TRY(cudaMemsetAsync(tc_status, 0, (size_t)np * sizeof(int32_t), st), err, cap);
+  int tc_rc = 0;
   auto update = [&](int k, const std::vector<int32_t>& off, const int32_t* dtiles,
                     const int32_t* dslots, int op) {
     const int n = off[k + 1] - off[k];
+    if (tc) {
+      if (tc_rc == 0)
+        tc_rc = solve_tc_update(k, n, dtiles + off[k], dslots + off[k], op, np, L, P, a->factor,
+                                W, Y, tc_status, st, err, cap);
+      return;
+    }
     dim3 g((unsigned)(n * rowblocks * ncs + kCopyBlocks), np);
     count_launches(1);
     if (op == kPlain)
@@ -205,6 +218,7 @@ int run_solve(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t
       update(k, P->ll_off, P->d_ll_tile, P->d_ll_slot, kConjT);
     }
   }
+  if (tc_rc) return tc_rc;
   return launch_check(err, cap, "solve");
 }
 
@@ -402,7 +416,30 @@ extern "C" {
 
 size_t aosb_solve_scratch_bytes(const aosb_plan_t* P, int32_t np, int32_t nrhs) {
   if (P == nullptr || np <= 0 || nrhs <= 0) return 0;
-  return (size_t)np * (size_t)P->T * (size_t)nrhs * sizeof(float2);
+  // diagonal results, then one status word per pencil for the tensor-core
+  // updates
+  return (size_t)np * (size_t)P->T * (size_t)nrhs * sizeof(float2) + (size_t)np * sizeof(int32_t);
+}
+
+int aosb_solve_check(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* err, size_t cap) {
+  using aosb::set_error;
+  if (P == nullptr || a == nullptr || a->scratch == nullptr)
+    return set_error(err, cap, AOSB_ERR_NULL, "null argument");
+  if (a->n_pencils <= 0 || a->n_pencils > 65535 || a->n_rhs <= 0)
+    return set_error(err, cap, AOSB_ERR_BATCH, "invalid pencil or right-hand-side count");
+  cudaStream_t st = (cudaStream_t)a->stream;
+  AOSB_CUDA_TRY(cudaStreamSynchronize(st), err, cap);
+  if (P->T != 128 || (a->flags & AOSB_SOLVE_TENSOR_CORES) == 0) return 0;
+  std::vector<int32_t> host((size_t)a->n_pencils);
+  const unsigned char* words =
+      (const unsigned char*)a->scratch + (size_t)a->n_pencils * P->T * a->n_rhs * sizeof(float2);
+  AOSB_CUDA_TRY(cudaMemcpy(host.data(), words, host.size() * sizeof(int32_t),
+                           cudaMemcpyDeviceToHost), err, cap);
+  for (size_t i = 0; i < host.size(); ++i)
+    if (host[i] != 0)
+      return set_error(err, cap, host[i], "tensor-core solve update of pencil %zu gave up a bounded "
+                       "wait (status %d)", i, host[i]);
+  return 0;
 }
 
 int aosb_solve(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* err, size_t cap) {

@@ -653,8 +653,11 @@ class BandEngine:
         need = native.library().aosb_solve_scratch_bytes(self.plan.handle, np_, L)
         if self._solve_scratch is None or self._solve_scratch.numel() < need:
             self._solve_scratch = torch.empty(max(need, 16), dtype=torch.uint8, device=self.device)
+        mixed_tc = (self.engine.precision == "mixed" and self.engine.tensor_cores
+                    and self.engine.tensor_core_solves and self.plan.info.tile == 128)
+        flags = native.SOLVE_TENSOR_CORES if mixed_tc else 0
         sa = native.SolveArgs(native.ABI_VERSION, native.C.sizeof(native.SolveArgs), np_, L,
-                              adjoint, 0, factor.data_ptr(), pivots.data_ptr(), wn.data_ptr(),
+                              adjoint, flags, factor.data_ptr(), pivots.data_ptr(), wn.data_ptr(),
                               self._solve_scratch.data_ptr(), st)
         for it in range(steps + 1):
             src = b if it == 0 else rr
@@ -665,6 +668,8 @@ class BandEngine:
                         xn.data_ptr(), 1 if it > 0 else 0, st)
             if it < steps:
                 self._residual(n, L, np_, hvals, svals, pk, z, b, xn, rr, st)
+        if flags:
+            native.call("aosb_solve_check", self.plan.handle, native.C.byref(sa))
 
     residual_kernel = "blocks"   # "blocks" (rows of one atom share x loads) or "rows"
 

@@ -24,6 +24,7 @@ ERROR_CAPACITY = 512
 PRECISION_PLAIN = 0
 PRECISION_BF16X3 = 1
 PRECISION_BF16X3_FP32_PANELS = 2
+SOLVE_TENSOR_CORES = 1
 
 STATUS_NAMES = {
     10: "ABI mismatch", 11: "dimensions", 12: "batch", 13: "null pointer",
@@ -59,7 +60,7 @@ class FactorArgs(C.Structure):
 
 class SolveArgs(C.Structure):
     _fields_ = [("abi_version", c_u32), ("struct_size", c_u32), ("n_pencils", c_i32),
-                ("n_rhs", c_i32), ("adjoint", c_i32), ("reserved", c_i32), ("factor", c_vp),
+                ("n_rhs", c_i32), ("adjoint", c_i32), ("flags", c_i32), ("factor", c_vp),
                 ("pivots", c_vp), ("work", c_vp), ("scratch", c_vp), ("stream", c_vp)]
 
 
@@ -119,6 +120,7 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_factor": (C.c_int, [c_vp, C.POINTER(FactorArgs), C.c_char_p, c_sz]),
     "aosb_solve": (C.c_int, [c_vp, C.POINTER(SolveArgs), C.c_char_p, c_sz]),
     "aosb_solve_scratch_bytes": (c_sz, [c_vp, c_i32, c_i32]),
+    "aosb_solve_check": (C.c_int, [c_vp, C.POINTER(SolveArgs), C.c_char_p, c_sz]),
     "aosb_gather_rhs": (C.c_int, [c_vp, c_i32, c_i32, c_vp, c_i64, c_vp, c_vp, C.c_char_p, c_sz]),
     "aosb_scatter_solution": (C.c_int, [c_vp, c_i32, c_i32, c_vp, c_vp, c_i32, c_vp,
                                         C.c_char_p, c_sz]),

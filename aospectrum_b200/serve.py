@@ -18,8 +18,9 @@ rejected with ``InputError``.
 
 Continuous batching: every admitted request is cut into work units of
 ``kpoints_per_unit`` k points.  ``slots`` worker threads, each with its own
-CUDA stream, take units round-robin over the admitted requests, so units of
-different requests run concurrently on the device and a request that
+CUDA stream, take units round-robin over the admitted requests (one unit of
+a request at a time: its engine and working set serve one stream), so units
+of different requests run concurrently on the device and a request that
 arrives while others are running starts as soon as a slot and memory free
 up.  A unit's numerics do not depend on what else runs: each pencil is
 factored and solved on its own, so a request's eigenvalues are the same
@@ -303,7 +304,9 @@ class BandServer:
         n = len(self._active)
         for j in range(n):
             act = self._active[(start + j) % n]
-            if act.units and act.failed is None:
+            # one unit in flight per request: a request's engine (and its
+            # scratch buffers and working set) serves one stream at a time
+            if act.units and act.failed is None and act.in_flight == 0:
                 return act, act.units.popleft()
         return None
 

@@ -280,14 +280,20 @@ int aosb_factor(const aosb_plan_t *plan, const aosb_factor_args_v1 *args,
  * shift of a contour node pair reuses one factorization this way).
  * work: device [n_pencils][n_pad][n_rhs] complex64, overwritten.
  * scratch: device, aosb_solve_scratch_bytes(plan, n_pencils, n_rhs).
+ * flags: AOSB_SOLVE_TENSOR_CORES (tile 128) runs the off-diagonal tile
+ * updates on the tensor cores in split BF16 (FP32 accumulation); 0 keeps
+ * them in FP32 SIMT.  The tensor-core updates bound their waits; after the
+ * solves, aosb_solve_check synchronizes the stream and reports a timeout.
  * ------------------------------------------------------------------------ */
+#define AOSB_SOLVE_TENSOR_CORES 1
+
 typedef struct {
   uint32_t abi_version;
   uint32_t struct_size;
   int32_t n_pencils;
   int32_t n_rhs;
   int32_t adjoint;
-  int32_t reserved;
+  int32_t flags;
   const float *factor;
   const int32_t *pivots;
   aosb_complex64 *work;
@@ -298,6 +304,12 @@ typedef struct {
 size_t aosb_solve_scratch_bytes(const aosb_plan_t *plan, int32_t n_pencils, int32_t n_rhs);
 int aosb_solve(const aosb_plan_t *plan, const aosb_solve_args_v1 *args,
                char *err, size_t err_cap);
+/* Synchronizes args->stream and returns AOSB_ERR_TIMEOUT when a
+ * tensor-core update of an aosb_solve call with these args gave up on a
+ * bounded wait (status words kept in the scratch block, cleared by each
+ * aosb_solve). */
+int aosb_solve_check(const aosb_plan_t *plan, const aosb_solve_args_v1 *args,
+                     char *err, size_t err_cap);
 
 /* work[p][i][:] = complex64(src[p*src_stride + perm[i]*n_rhs + :]), zero for
  * padding rows (src: device complex128 [.][n][n_rhs]). */

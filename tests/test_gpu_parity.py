@@ -88,7 +88,8 @@ def _pencil_case(bundle, k, torch, tile, ordering="nested_dissection"):
     return dev, plan, h, s
 
 
-def _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=0, adjoint=0, steps=0):
+def _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=0, adjoint=0, steps=0,
+                  flags=0):
     """Factor len(shifts) pencils of one k and solve with rhs (n x L)."""
     from aospectrum_b200 import native
 
@@ -118,8 +119,9 @@ def _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=0, adjoint=0, s
     w = torch.empty((P, info.n_pad, L), dtype=torch.complex64, device=dv)
     scratch = torch.empty(max(16, lib.aosb_solve_scratch_bytes(plan.handle, P, L)),
                           dtype=torch.uint8, device=dv)
-    sa = native.SolveArgs(native.ABI_VERSION, native.C.sizeof(native.SolveArgs), P, L, adjoint, 0,
-                          factor.data_ptr(), piv.data_ptr(), w.data_ptr(), scratch.data_ptr(), st)
+    sa = native.SolveArgs(native.ABI_VERSION, native.C.sizeof(native.SolveArgs), P, L, adjoint,
+                          flags, factor.data_ptr(), piv.data_ptr(), w.data_ptr(),
+                          scratch.data_ptr(), st)
     zz = torch.conj_physical(z) if adjoint else z
     for it in range(steps + 1):
         src = b if it == 0 else r
@@ -131,6 +133,7 @@ def _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=0, adjoint=0, s
             native.call("aosb_shifted_residual", n, L, P, dev.d_indptr, dev.d_indices,
                         h.data_ptr(), s.data_ptr(), dev.nnz, pk.data_ptr(), zz.data_ptr(),
                         b.data_ptr(), n * L, x.data_ptr(), r.data_ptr(), st)
+    native.call("aosb_solve_check", plan.handle, native.C.byref(sa))
     torch.cuda.synchronize()
     return x.cpu().numpy()
 
@@ -169,22 +172,23 @@ def test_plain_factor_solve_matches_superlu(case, tile, ordering, torch):
         plan.close()
 
 
-@pytest.mark.parametrize("precision", [1, 2])
+@pytest.mark.parametrize("precision,flags", [(1, 0), (2, 0), (1, 1)])
 @pytest.mark.parametrize("case", ["small2d", "c1"])
-def test_tensor_core_factor_matches_superlu(case, precision, torch):
+def test_tensor_core_factor_matches_superlu(case, precision, flags, torch):
     """Split-BF16 tcgen05 Schur updates (precision 1: tensor-core panels
-    too; 2: FP32 SIMT panels): unrefined solves within 1e-3, FP64
-    refinement to 1e-9, both directions."""
+    too; 2: FP32 SIMT panels; flags 1: tensor-core solve updates): unrefined
+    solves within 1e-3, FP64 refinement to 1e-9, both directions."""
     b = getattr(bundles, case)()
     dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[1], torch, 128)
     try:
         rng = np.random.default_rng(3)
         rhs = (rng.standard_normal((dev.n, 8)) + 1j * rng.standard_normal((dev.n, 8)))
         shifts = [-2.6 + 0.004j, -2.4 + 0.04j, -1.0 + 0.5j]
-        x0 = _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=precision)
+        x0 = _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=precision,
+                           flags=flags)
         for adjoint in (0, 1):
             x = _factor_solve(dev, plan, h, s, shifts, rhs, torch, precision=precision,
-                              adjoint=adjoint, steps=3)
+                              adjoint=adjoint, steps=3, flags=flags)
             for p, z in enumerate(shifts):
                 ref = _splu_reference(dev, h, s, z, rhs, adjoint=bool(adjoint))
                 if adjoint == 0:

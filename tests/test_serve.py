@@ -43,6 +43,9 @@ class SlowOracle(OracleEngine):
         with SlowOracle.lock:
             SlowOracle.running += 1
             SlowOracle.peak = max(SlowOracle.peak, SlowOracle.running)
+            # an engine (one request) must never serve two units at once
+            assert not getattr(self, "_busy", False), "engine used by two units at once"
+            self._busy = True
         try:
             time.sleep(0.02)
             if id(self.bundle) in SlowOracle.failing:
@@ -51,6 +54,7 @@ class SlowOracle(OracleEngine):
         finally:
             with SlowOracle.lock:
                 SlowOracle.running -= 1
+                self._busy = False
 
 
 def _server(budget, footprints, slots=3, **kw):
