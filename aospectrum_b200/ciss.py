@@ -94,6 +94,11 @@ class EngineSettings:
     tensor_core_solves: with tensor cores, run the off-diagonal tile
         updates of the triangular sweeps in split BF16 too (FP64
         refinement recovers the accuracy); False keeps them in FP32 SIMT.
+    cuda_graphs: capture each batch's triangular sweeps (hundreds of
+        launches per solve) into a CUDA graph on first use and replay it.
+    autotune: with tile 0, time the candidate tile plans (tile edge x
+        ordering) on the device for this pattern and keep the fastest
+        (aospectrum_b200.autotune); False picks by size and flop count.
     """
 
     precision: str = "mixed"
@@ -105,6 +110,8 @@ class EngineSettings:
     tensor_cores: bool = True
     tensor_core_panels: bool = True
     tensor_core_solves: bool = False
+    autotune: bool = False
+    cuda_graphs: bool = False
 
     def __post_init__(self) -> None:
         if self.precision not in PRECISIONS:

@@ -32,7 +32,6 @@
 #include "tc_common.cuh"
 
 #include <cuda.h>
-#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -520,35 +519,9 @@ static int side_stream(cudaStream_t main, cudaStream_t* out, char* err, size_t c
 
 // Tensor map of the factor storage as a [rows][T] FP32 matrix (each tile is
 // 2 planes x T rows), 32 x 32 boxes, 128-byte swizzle: the destination of
-// the epilogue's bulk reduce-add.
+// the epilogue's bulk reduce-add and store.
 static int factor_tensor_map(void* factor, int64_t rows, CUtensorMap* map, char* err, size_t cap) {
-  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-  static std::mutex mu;
-  {
-    std::lock_guard<std::mutex> lock(mu);
-    if (encode == nullptr) {
-      cudaDriverEntryPointQueryResult q;
-      void* fn = nullptr;
-      cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
-      if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || fn == nullptr)
-        return set_error(err, cap, AOSB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
-      encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-    }
-  }
-  if (((uintptr_t)factor & 15) != 0)
-    return set_error(err, cap, AOSB_ERR_ARGUMENT, "factor storage must be 16-byte aligned");
-  if (rows <= 0 || rows > (int64_t)INT32_MAX)
-    return set_error(err, cap, AOSB_ERR_SIZE, "factor storage too large for 32-bit TMA rows");
-  cuuint64_t gdim[2] = {(cuuint64_t)kTcT, (cuuint64_t)rows};
-  cuuint64_t gstride[1] = {(cuuint64_t)kTcT * sizeof(float)};
-  cuuint32_t box[2] = {32, 32};
-  cuuint32_t estride[2] = {1, 1};
-  CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, factor, gdim, gstride, box, estride,
-                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS)
-    return set_error(err, cap, AOSB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
-  return 0;
+  return encode_f32_2d(factor, kTcT, (uint64_t)rows, 32, 32, true, map, err, cap);
 }
 
 int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {

@@ -558,6 +558,7 @@ int aosb_plan_export_slots(const aosb_plan_t* p, int32_t* slot) {
 
 void aosb_plan_destroy(aosb_plan_t* p) {
   if (p == nullptr) return;
+  aosb::solve_graphs_forget(p);
   aosb::plan_free_device(p);
   delete p;
 }

@@ -37,4 +37,5 @@ struct aosb_plan {
 namespace aosb {
 int plan_upload(aosb_plan* p, char* err, size_t cap);
 void plan_free_device(aosb_plan* p);
+void solve_graphs_forget(const aosb_plan* p);
 }  // namespace aosb

@@ -14,11 +14,20 @@
 // kernel for every off-diagonal tile of that step.
 #include "plan.h"
 #include "cgemm.cuh"
+#include "tc_common.cuh"
+
+#include <cuda_bf16.h>
+
+#include <mutex>
+#include <vector>
 
 namespace aosb {
+int solve_graph(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t cap,
+                int (*direct)(const aosb_plan*, const aosb_solve_args_v1*, char*, size_t));
 int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, int op, int np,
                     int nrhs, const aosb_plan* P, const float* factor, float2* work,
-                    const float2* ytmp, int32_t* status, cudaStream_t st, char* err, size_t cap);
+                    const float2* ytmp, const unsigned char* ystaged, int32_t* status,
+                    cudaStream_t st, char* err, size_t cap);
 namespace {
 
 constexpr int kThreads = 256;
@@ -43,7 +52,8 @@ __global__ void __launch_bounds__(kThreads) solve_diag_kernel(int k, int nrhs, i
                                                               const float* __restrict__ factor,
                                                               const int32_t* __restrict__ pivots,
                                                               const float2* __restrict__ work,
-                                                              float2* __restrict__ ytmp) {
+                                                              float2* __restrict__ ytmp,
+                                                              unsigned char* __restrict__ ystaged) {
   constexpr int BM = 32, BN = 32, TM = 2, TN = 2;
   static_assert((BM / TM) * (BN / TN) == 256, "layout");
   __shared__ CgemmSmem<BM, BN> sm[2];
@@ -91,6 +101,21 @@ __global__ void __launch_bounds__(kThreads) solve_diag_kernel(int k, int nrhs, i
       if (col >= nrhs) continue;
       const int row = OP == kLinvH ? pv[r] : r;
       Y[(size_t)row * nrhs + col] = make_float2(accr[i][j], acci[i][j]);
+      if (ystaged != nullptr) {
+        // the same value as the tensor-core update's B operand (strip of 32
+        // columns): four BF16 planes, x = hi + lo
+        const int strips = (nrhs + tc::kSolveNS - 1) / tc::kSolveNS;
+        unsigned char* sp = ystaged + ((size_t)p * strips + col / tc::kSolveNS) * tc::kSolveBBytes;
+        const int n = col % tc::kSolveNS;
+        const __nv_bfloat16 rh = __float2bfloat16_rn(accr[i][j]);
+        const __nv_bfloat16 ih = __float2bfloat16_rn(acci[i][j]);
+        *reinterpret_cast<__nv_bfloat16*>(sp + tc::solve_b_offset(n, row, 0)) = rh;
+        *reinterpret_cast<__nv_bfloat16*>(sp + tc::solve_b_offset(n, row, 1)) =
+            __float2bfloat16_rn(accr[i][j] - __bfloat162float(rh));
+        *reinterpret_cast<__nv_bfloat16*>(sp + tc::solve_b_offset(n, row, 2)) = ih;
+        *reinterpret_cast<__nv_bfloat16*>(sp + tc::solve_b_offset(n, row, 3)) =
+            __float2bfloat16_rn(acci[i][j] - __bfloat162float(ih));
+      }
     }
 }
 
@@ -166,18 +191,25 @@ int run_solve(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t
   const int rowblocks = T / BM;
   float2* W = (float2*)a->work;
   float2* Y = (float2*)a->scratch;
+  const bool tc = T == 128 && (a->flags & AOSB_SOLVE_TENSOR_CORES) != 0;
+  // scratch: Y [np][T][L] complex64 | status [np] int32 | (tensor cores) Y
+  // as BF16 B-operand planes [np][strips][32 KB], 128-byte aligned
+  int32_t* tc_status = (int32_t*)((unsigned char*)a->scratch + (size_t)np * T * L * sizeof(float2));
+  unsigned char* ystaged = nullptr;
+  if (tc) {
+    const size_t off = (size_t)np * T * L * sizeof(float2) + (size_t)np * sizeof(int32_t);
+    ystaged = (unsigned char*)a->scratch + ((off + 127) & ~(size_t)127);
+  }
   auto diag = [&](int k, int op) {
     count_launches(1);
     dim3 g(ncs, T / 32, np);
     switch (op) {
-      case kLinv: solve_diag_kernel<T, kLinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y); break;
-      case kUinv: solve_diag_kernel<T, kUinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y); break;
-      case kUinvH: solve_diag_kernel<T, kUinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y); break;
-      default: solve_diag_kernel<T, kLinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y); break;
+      case kLinv: solve_diag_kernel<T, kLinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
+      case kUinv: solve_diag_kernel<T, kUinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
+      case kUinvH: solve_diag_kernel<T, kUinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
+      default: solve_diag_kernel<T, kLinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
     }
   };
-  const bool tc = T == 128 && (a->flags & AOSB_SOLVE_TENSOR_CORES) != 0;
-  int32_t* tc_status = (int32_t*)((unsigned char*)a->scratch + (size_t)np * T * L * sizeof(float2));
   if (tc) AOSB_CUDA_TRY(cudaMemsetAsync(tc_status, 0, (size_t)np * sizeof(int32_t), st), err, cap);
   int tc_rc = 0;
   auto update = [&](int k, const std::vector<int32_t>& off, const int32_t* dtiles,
@@ -186,7 +218,7 @@ int run_solve(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t
     if (tc) {
       if (tc_rc == 0)
         tc_rc = solve_tc_update(k, n, dtiles + off[k], dslots + off[k], op, np, L, P, a->factor,
-                                W, Y, tc_status, st, err, cap);
+                                W, Y, ystaged, tc_status, st, err, cap);
       return;
     }
     dim3 g((unsigned)(n * rowblocks * ncs + kCopyBlocks), np);
@@ -410,15 +442,113 @@ __global__ void __launch_bounds__(kResWarps * 32) shifted_residual_blocks_kernel
 }
 
 }  // namespace
+
+// CUDA-graph replay of whole solves.  The launch sequence of one aosb_solve
+// (a diagonal and an update launch per tile step and sweep) depends only on
+// the plan, the batch shape, the flags and the buffer addresses, so it is
+// captured once per such key and replayed with cudaGraphLaunch afterwards.
+// Graphs referring to a plan are dropped when the plan is destroyed.
+struct SolveGraphKey {
+  const aosb_plan* P;
+  int device, np, L, adjoint, flags;
+  const void *factor, *pivots, *work, *scratch;
+  bool operator==(const SolveGraphKey& o) const {
+    return P == o.P && device == o.device && np == o.np && L == o.L && adjoint == o.adjoint &&
+           flags == o.flags && factor == o.factor && pivots == o.pivots && work == o.work &&
+           scratch == o.scratch;
+  }
+};
+struct SolveGraph {
+  SolveGraphKey key;
+  cudaGraphExec_t exec;
+  size_t kernels;
+  uint64_t last_use;
+};
+static std::mutex g_graph_mu;
+static std::vector<SolveGraph> g_graphs;
+static uint64_t g_graph_clock = 0;
+constexpr size_t kMaxSolveGraphs = 32;
+
+void solve_graphs_forget(const aosb_plan* P) {
+  std::lock_guard<std::mutex> lock(g_graph_mu);
+  for (size_t i = 0; i < g_graphs.size();) {
+    if (g_graphs[i].key.P == P) {
+      cudaGraphExecDestroy(g_graphs[i].exec);
+      g_graphs[i] = g_graphs.back();
+      g_graphs.pop_back();
+    } else {
+      ++i;
+    }
+  }
+}
+
+int solve_graph(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t cap,
+                int (*direct)(const aosb_plan*, const aosb_solve_args_v1*, char*, size_t)) {
+  cudaStream_t st = (cudaStream_t)a->stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  AOSB_CUDA_TRY(cudaStreamIsCapturing(st, &cs), err, cap);
+  if (cs != cudaStreamCaptureStatusNone || st == nullptr) return direct(P, a, err, cap);
+  int device = 0;
+  AOSB_CUDA_TRY(cudaGetDevice(&device), err, cap);
+  const SolveGraphKey key{P, device, a->n_pencils, a->n_rhs, a->adjoint, a->flags,
+                          a->factor, a->pivots, a->work, a->scratch};
+  {
+    std::lock_guard<std::mutex> lock(g_graph_mu);
+    for (auto& g : g_graphs) {
+      if (g.key == key) {
+        g.last_use = ++g_graph_clock;
+        AOSB_CUDA_TRY(cudaGraphLaunch(g.exec, st), err, cap);
+        count_launches(g.kernels);
+        return 0;
+      }
+    }
+  }
+  // capture (thread-local mode: other threads keep issuing CUDA calls)
+  AOSB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), err, cap);
+  const int rc = direct(P, a, err, cap);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &graph);
+  if (rc != 0) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess)
+    return set_error(err, cap, AOSB_ERR_CUDA, "solve capture failed: %s", cudaGetErrorString(e));
+  size_t nodes = 0;
+  cudaGraphGetNodes(graph, nullptr, &nodes);
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess)
+    return set_error(err, cap, AOSB_ERR_CUDA, "solve graph instantiate: %s", cudaGetErrorString(ei));
+  AOSB_CUDA_TRY(cudaGraphLaunch(exec, st), err, cap);
+  std::lock_guard<std::mutex> lock(g_graph_mu);
+  if (g_graphs.size() >= kMaxSolveGraphs) {
+    size_t old = 0;
+    for (size_t i = 1; i < g_graphs.size(); ++i)
+      if (g_graphs[i].last_use < g_graphs[old].last_use) old = i;
+    cudaGraphExecDestroy(g_graphs[old].exec);
+    g_graphs[old] = g_graphs.back();
+    g_graphs.pop_back();
+  }
+  g_graphs.push_back({key, exec, nodes, ++g_graph_clock});
+  return 0;
+}
+
 }  // namespace aosb
 
 extern "C" {
 
 size_t aosb_solve_scratch_bytes(const aosb_plan_t* P, int32_t np, int32_t nrhs) {
   if (P == nullptr || np <= 0 || nrhs <= 0) return 0;
-  // diagonal results, then one status word per pencil for the tensor-core
-  // updates
-  return (size_t)np * (size_t)P->T * (size_t)nrhs * sizeof(float2) + (size_t)np * sizeof(int32_t);
+  // diagonal results, one status word per pencil for the tensor-core
+  // updates and (tile 128) the diagonal results as BF16 B-operand planes
+  size_t bytes = (size_t)np * (size_t)P->T * (size_t)nrhs * sizeof(float2) + (size_t)np * sizeof(int32_t);
+  if (P->T == 128) {
+    const size_t strips = (size_t)((nrhs + aosb::tc::kSolveNS - 1) / aosb::tc::kSolveNS);
+    bytes = ((bytes + 127) & ~(size_t)127) + (size_t)np * strips * aosb::tc::kSolveBBytes;
+  }
+  return bytes;
 }
 
 int aosb_solve_check(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* err, size_t cap) {
@@ -442,6 +572,15 @@ int aosb_solve_check(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* er
   return 0;
 }
 
+static int solve_direct(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* err, size_t cap) {
+  switch (P->T) {
+    case 32: return aosb::run_solve<32>(P, a, err, cap);
+    case 64: return aosb::run_solve<64>(P, a, err, cap);
+    case 128: return aosb::run_solve<128>(P, a, err, cap);
+  }
+  return aosb::set_error(err, cap, AOSB_ERR_UNSUPPORTED, "unsupported tile size");
+}
+
 int aosb_solve(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* err, size_t cap) {
   using aosb::set_error;
   if (P == nullptr || a == nullptr) return set_error(err, cap, AOSB_ERR_NULL, "null argument");
@@ -452,12 +591,8 @@ int aosb_solve(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* err, siz
   if (a->factor == nullptr || a->pivots == nullptr || a->work == nullptr || a->scratch == nullptr)
     return set_error(err, cap, AOSB_ERR_NULL, "required pointer is null");
   if (!P->uploaded) return set_error(err, cap, AOSB_ERR_ARGUMENT, "call aosb_plan_upload first");
-  switch (P->T) {
-    case 32: return aosb::run_solve<32>(P, a, err, cap);
-    case 64: return aosb::run_solve<64>(P, a, err, cap);
-    case 128: return aosb::run_solve<128>(P, a, err, cap);
-  }
-  return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "unsupported tile size");
+  if ((a->flags & AOSB_SOLVE_GRAPH) == 0) return solve_direct(P, a, err, cap);
+  return aosb::solve_graph(P, a, err, cap, solve_direct);
 }
 
 int aosb_gather_rhs(const aosb_plan_t* P, int32_t np, int32_t nrhs, const aosb_complex128* src,

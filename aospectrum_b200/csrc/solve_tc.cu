@@ -1,24 +1,30 @@
 // Tensor-core (tcgen05) update step of the block-RHS triangular sweeps for
 // tile 128: X_i -= op(F) Y for every listed tile F of the step, with
 // op(F) = F (plain) or F^H (adjoint sweeps) and Y the step's diagonal
-// result (T x n_rhs complex64, computed by the SIMT diagonal kernel).
+// result (T x n_rhs complex64, written by the SIMT diagonal kernel together
+// with its split-BF16 copy, the B operand: four BF16 planes re_hi, re_lo,
+// im_hi, im_lo per 32-column RHS strip).
 //
-// One CTA (4 warps) per (tile, 64-column RHS strip, pencil):
-//   * the Y strip is split into four BF16 planes (re_hi, re_lo, im_hi,
-//     im_lo; x = hi + lo) as the K-major B operand (N = strip columns
-//     rounded up to 16, K = 128) in shared memory;
-//   * the FP32 factor tile is read from HBM in 16-wide K slabs, split the
-//     same way into the K-major A operand (M = 128) in a two-slab ring, and
-//     for each slab one thread issues 12 tcgen05.mma.kind::f16 into two
-//     FP32 TMEM accumulators (the split-BF16 complex product of the
-//     factorization: hi*hi + hi*lo + lo*hi per real product);
-//   * each warp reads its 32 rows of the accumulators with tcgen05.ld and
-//     subtracts them from X_i.
-// The conversion of slab s+1 overlaps the MMAs of slab s; each slab buffer
-// is rewritten only after the tcgen05.commit of the MMAs that read it has
-// arrived on its mbarrier.  Every wait is bounded: on expiry the CTA
-// records AOSB_ERR_TIMEOUT in the pencil status, skips the rest, waits
-// (bounded) for MMAs in flight and frees its TMEM.
+// Persistent and warp specialized; each CTA walks the step's (pencil,
+// strip, tile) items with stride gridDim.x:
+//   warp 0 lane 0   producer: per item one bulk copy of the Y strip planes
+//                   (32 KB) into a two-buffer ring, and per 16-wide K slab two
+//                   TMA tensor loads of the FP32 factor tile (real and
+//                   imaginary plane boxes) into a kRawStages-deep ring;
+//   warps 2-5       converters: split each FP32 slab into the four BF16
+//                   planes of the K-major A operand (M = 128) in a
+//                   kAStages-deep ring (op(F) = F^H reads the slab transposed
+//                   and negates the imaginary part);
+//   warp 1 lane 0   MMA issuer: 12 tcgen05.mma.kind::f16 (M = 128, N = strip
+//                   width rounded up to 16) per slab into one of two TMEM
+//                   accumulator pairs (re, im): hi*hi + hi*lo + lo*hi per real
+//                   product, FP32 accumulation;
+//   warps 6-9       epilogue: tcgen05.ld of the accumulator (warp w reads
+//                   lanes 32 (w % 4) ..), X_i -= acc.
+// Two accumulator pairs let one item's epilogue overlap the next item's
+// MMAs.  Every mbarrier wait is bounded: on expiry the CTA records
+// AOSB_ERR_TIMEOUT in the pencil status and stops; a CTA that stops waits
+// (bounded) for its own copies and MMAs in flight and frees its TMEM.
 #include "plan.h"
 #include "tc_common.cuh"
 
@@ -30,37 +36,40 @@ namespace {
 using namespace tc;
 
 constexpr int kT = 128;
-constexpr int kNS = 64;                    // RHS columns per CTA
+constexpr int kNS = kSolveNS;              // RHS columns per item (32)
 constexpr int kSK = 16;                    // K per slab
 constexpr int kSlabsS = kT / kSK;          // 8
-constexpr int kSThreads = 128;
-constexpr int kACols = 2 * kNS;            // TMEM columns: re [0, kNS), im [kNS, 2 kNS)
-constexpr int kAPlane = kT * kSK * 2;      // 4096 bytes: one plane of one A slab
+constexpr int kRawStages = 4;              // FP32 slab ring
+constexpr int kAStages = 3;                // BF16 A slab ring
+constexpr int kConvWarps = 4, kEpiWarps = 4;
+constexpr int kConvWarp0 = 2, kEpiWarp0 = kConvWarp0 + kConvWarps;  // 2, 6
+constexpr int kSThreads = (kEpiWarp0 + kEpiWarps) * 32;              // 320
+constexpr int kACols = 4 * kNS;            // two accumulator pairs (re, im) = 128 columns
+constexpr int kAPlane = kT * kSK * 2;      // 4096 bytes: one BF16 plane of one A slab
 constexpr int kASlab = 4 * kAPlane;        // 16 KB
-constexpr int kBPlaneSlab = kNS * kSK * 2;  // 2048 bytes
-constexpr int kBSlab = 4 * kBPlaneSlab;    // 8 KB
+constexpr int kRawPlane = kT * kSK;        // floats in one FP32 plane box of a slab
+constexpr uint32_t kRawBytes = 2 * kRawPlane * sizeof(float);  // 16 KB per slab
 constexpr int kCopyCtas = 4;
 
 enum SolveOp { kOpPlain = 0, kOpConjT = 1 };
 
 struct SShared {
-  alignas(1024) unsigned char b[kSlabsS][kBSlab];   // 64 KB
-  alignas(1024) unsigned char a[2][kASlab];          // 32 KB
-  uint64_t done[2];
+  alignas(128) float raw[kRawStages][2][kRawPlane];   // 64 KB
+  alignas(128) unsigned char a[kAStages][kASlab];      // 48 KB
+  alignas(128) unsigned char b[2][kSolveBBytes];       // 64 KB
+  uint64_t raw_full[kRawStages], raw_empty[kRawStages];
+  uint64_t a_full[kAStages], a_empty[kAStages];
+  uint64_t b_full[2], b_empty[2];
+  uint64_t acc_full[2], acc_empty[2];
   uint32_t tmem_base;
   int failed;
 };
 
 // K-major no-swizzle core-matrix layout (8 rows x 16 bytes), the two 8-wide
-// K halves of a slab `rows / 8 * 128` bytes apart.
+// K halves of a slab (kT / 8) * 128 bytes apart.
 __device__ __forceinline__ uint32_t a_off(int m, int k, int plane) {
   return (uint32_t)(plane * kAPlane + (k / 8) * ((kT / 8) * 128) + (m / 8) * 128 + (m % 8) * 16 +
                     (k % 8) * 2);
-}
-__device__ __forceinline__ uint32_t b_off(int n, int k, int plane) {
-  const int slab = k / kSK, kk = k % kSK;
-  return (uint32_t)(slab * kBSlab + plane * kBPlaneSlab + (kk / 8) * ((kNS / 8) * 128) +
-                    (n / 8) * 128 + (n % 8) * 16 + (kk % 8) * 2);
 }
 
 __device__ __forceinline__ void split2(float x0, float x1, __nv_bfloat162& hi, __nv_bfloat162& lo) {
@@ -71,37 +80,63 @@ __device__ __forceinline__ void split2(float x0, float x1, __nv_bfloat162& hi, _
   lo.y = __float2bfloat16_rn(x1 - __bfloat162float(h1));
 }
 
+struct ItemOf {
+  int p, strip, tile_idx;
+};
+__device__ __forceinline__ ItemOf item_of(int it, int n_items, int strips) {
+  const int per_pencil = n_items * strips;
+  ItemOf r;
+  r.p = it / per_pencil;
+  const int rem = it % per_pencil;
+  r.strip = rem / n_items;
+  r.tile_idx = rem % n_items;
+  return r;
+}
+
+__device__ __forceinline__ void fail(SShared& sh, int32_t* status, int p) {
+  sh.failed = 1;
+  atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
+}
+
 template <int OP>
-__global__ void __launch_bounds__(kSThreads) solve_tc_kernel(
-    int k, int n_items, int nrhs, int64_t n_pad, const int32_t* __restrict__ tiles,
-    const int32_t* __restrict__ slots, int64_t n_slots, const float* __restrict__ factor,
-    float2* __restrict__ work, const float2* __restrict__ ytmp, int32_t* __restrict__ status) {
-  const int p = blockIdx.y;
+__global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
+    int k, int n_items, int nrhs, int n_pencils, int64_t n_pad, const int32_t* __restrict__ tiles,
+    const int32_t* __restrict__ slots, int64_t n_slots, float2* __restrict__ work,
+    const float2* __restrict__ ytmp, const unsigned char* __restrict__ ystaged,
+    int32_t* __restrict__ status, const __grid_constant__ CUtensorMap fmap) {
   const int strips = (nrhs + kNS - 1) / kNS;
-  const int work_blocks = n_items * strips;
-  const float2* Y = ytmp + (size_t)p * kT * nrhs;
-  if ((int)blockIdx.x >= work_blocks) {
-    // copy-back CTAs: X_k = Y
-    const int cb = blockIdx.x - work_blocks;
-    float2* Xk = work + ((size_t)p * n_pad + (size_t)k * kT) * nrhs;
-    const int total = kT * nrhs;
-    for (int e = cb * kSThreads + threadIdx.x; e < total; e += kCopyCtas * kSThreads) Xk[e] = Y[e];
+  const int total = n_items * strips * n_pencils;
+  const int work_ctas = (int)gridDim.x - kCopyCtas;
+  if ((int)blockIdx.x >= work_ctas) {
+    // copy-back CTAs: X_k = Y for every pencil
+    const int cb = blockIdx.x - work_ctas;
+    const int per = kT * nrhs;
+    for (int64_t e = (int64_t)cb * blockDim.x + threadIdx.x; e < (int64_t)per * n_pencils;
+         e += (int64_t)kCopyCtas * blockDim.x) {
+      const int p = (int)(e / per), r = (int)(e % per);
+      work[((size_t)p * n_pad + (size_t)k * kT) * nrhs + r] = ytmp[(size_t)p * per + r];
+    }
     return;
   }
   extern __shared__ unsigned char dyn[];
   SShared& sh = *reinterpret_cast<SShared*>(
-      (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
-  const int item = blockIdx.x / strips, strip = blockIdx.x % strips;
-  const int c0 = strip * kNS;
-  const int ncols = nrhs - c0 < kNS ? nrhs - c0 : kNS;
-  const int n16 = (ncols + 15) & ~15;
-  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  const float* F = factor + ((size_t)p * (size_t)n_slots + (size_t)slots[item]) * (2 * kT * kT);
-  float2* Xi = work + ((size_t)p * n_pad + (size_t)tiles[item] * kT) * nrhs;
-
-  if (tid == 0) {
-    mbar_init(&sh.done[0], 1);
-    mbar_init(&sh.done[1], 1);
+      (reinterpret_cast<uintptr_t>(dyn) + 127) & ~(uintptr_t)127);
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kRawStages; ++s) {
+      mbar_init(&sh.raw_full[s], 1);
+      mbar_init(&sh.raw_empty[s], kConvWarps);
+    }
+    for (int s = 0; s < kAStages; ++s) {
+      mbar_init(&sh.a_full[s], kConvWarps);
+      mbar_init(&sh.a_empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&sh.b_full[b], 1);
+      mbar_init(&sh.b_empty[b], 1);
+      mbar_init(&sh.acc_full[b], 1);
+      mbar_init(&sh.acc_empty[b], kEpiWarps);
+    }
     sh.failed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -111,123 +146,194 @@ __global__ void __launch_bounds__(kSThreads) solve_tc_kernel(
                  "r"(kACols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // B operand: element (n, q) = Y[q][c0 + n], zero beyond the strip
-  for (int e = tid; e < kNS * (kT / 2); e += kSThreads) {
-    const int n = e % kNS, q = (e / kNS) * 2;
-    float2 y0 = make_float2(0.f, 0.f), y1 = y0;
-    if (n < ncols) {
-      y0 = Y[(size_t)q * nrhs + c0 + n];
-      y1 = Y[(size_t)(q + 1) * nrhs + c0 + n];
-    }
-    __nv_bfloat162 rh, rl, ih, il;
-    split2(y0.x, y1.x, rh, rl);
-    split2(y0.y, y1.y, ih, il);
-    unsigned char* b = &sh.b[0][0];
-    *reinterpret_cast<__nv_bfloat162*>(b + b_off(n, q, 0)) = rh;
-    *reinterpret_cast<__nv_bfloat162*>(b + b_off(n, q, 1)) = rl;
-    *reinterpret_cast<__nv_bfloat162*>(b + b_off(n, q, 2)) = ih;
-    *reinterpret_cast<__nv_bfloat162*>(b + b_off(n, q, 3)) = il;
-  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = sh.tmem_base;
-  const uint32_t id_pos = umma_idesc_mn(kT, n16, false), id_neg = umma_idesc_mn(kT, n16, true);
-  int issued = 0;  // slabs whose MMAs were committed
 
-  for (int s = 0; s < kSlabsS; ++s) {
-    const int buf = s & 1;
-    if (s >= 2) {
-      const bool ok = mbar_wait(&sh.done[buf], (uint32_t)(((s - 2) >> 1) & 1));
-      if (!ok && tid == 0) sh.failed = 1;
-    }
-    __syncthreads();
-    if (sh.failed) break;
-    unsigned char* a = sh.a[buf];
-    const int k0 = s * kSK;
-    // A operand slab: element (m, q) = F[m][k0 + q] or conj(F[k0 + q][m])
-    for (int e = tid; e < kT * (kSK / 2); e += kSThreads) {
-      int m, q;
-      float r0, r1, i0, i1;
-      if (OP == kOpPlain) {
-        m = e / (kSK / 2);
-        q = (e % (kSK / 2)) * 2;
-        const size_t o = (size_t)m * kT + k0 + q;
-        const float2 rr = *reinterpret_cast<const float2*>(F + o);
-        const float2 ii = *reinterpret_cast<const float2*>(F + kT * kT + o);
-        r0 = rr.x; r1 = rr.y; i0 = ii.x; i1 = ii.y;
-      } else {
-        m = e % kT;
-        q = (e / kT) * 2;
-        const size_t o0 = (size_t)(k0 + q) * kT + m, o1 = o0 + kT;
-        r0 = F[o0]; r1 = F[o1];
-        i0 = -F[kT * kT + o0]; i1 = -F[kT * kT + o1];
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      int g = 0;  // slab counter over all items of this CTA
+      int j = 0;  // item counter
+      for (int it = blockIdx.x; it < total && !sh.failed; it += work_ctas, ++j) {
+        const ItemOf w = item_of(it, n_items, strips);
+        const int bb = j & 1;
+        if (!mbar_wait(&sh.b_empty[bb], (uint32_t)(((j >> 1) & 1) ^ 1))) { fail(sh, status, w.p); break; }
+        mbar_expect_tx(&sh.b_full[bb], kSolveBBytes);
+        bulk_g2s(sh.b[bb], ystaged + ((size_t)w.p * strips + w.strip) * kSolveBBytes,
+                 kSolveBBytes, &sh.b_full[bb]);
+        const int64_t row0 = ((int64_t)w.p * n_slots + slots[w.tile_idx]) * (2 * kT);
+        bool ok = true;
+        for (int s = 0; s < kSlabsS; ++s, ++g) {
+          const int st = g % kRawStages;
+          if (!mbar_wait(&sh.raw_empty[st], (uint32_t)(((g / kRawStages) & 1) ^ 1))) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&sh.raw_full[st], kRawBytes);
+          if (OP == kOpPlain) {
+            tma_load_2d(sh.raw[st][0], &fmap, s * kSK, (int)row0, &sh.raw_full[st]);
+            tma_load_2d(sh.raw[st][1], &fmap, s * kSK, (int)(row0 + kT), &sh.raw_full[st]);
+          } else {
+            tma_load_2d(sh.raw[st][0], &fmap, 0, (int)(row0 + s * kSK), &sh.raw_full[st]);
+            tma_load_2d(sh.raw[st][1], &fmap, 0, (int)(row0 + kT + s * kSK), &sh.raw_full[st]);
+          }
+        }
+        if (!ok) { fail(sh, status, w.p); break; }
       }
-      __nv_bfloat162 rh, rl, ih, il;
-      split2(r0, r1, rh, rl);
-      split2(i0, i1, ih, il);
-      *reinterpret_cast<__nv_bfloat162*>(a + a_off(m, q, 0)) = rh;
-      *reinterpret_cast<__nv_bfloat162*>(a + a_off(m, q, 1)) = rl;
-      *reinterpret_cast<__nv_bfloat162*>(a + a_off(m, q, 2)) = ih;
-      *reinterpret_cast<__nv_bfloat162*>(a + a_off(m, q, 3)) = il;
     }
-    fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t sa = smem_u32(a), sb = smem_u32(sh.b[s]);
+  } else if (warp == 1) {
+    // ---------------------------------------------------------- MMA issuer
+    if (lane == 0) {
       const uint32_t alb = (kT / 8) * 128, blb = (kNS / 8) * 128;
-      uint64_t A[4], Bv[4];
+      int g = 0, j = 0;
+      for (int it = blockIdx.x; it < total && !sh.failed; it += work_ctas, ++j) {
+        const ItemOf w = item_of(it, n_items, strips);
+        const int ncols = nrhs - w.strip * kNS < kNS ? nrhs - w.strip * kNS : kNS;
+        const int n16 = (ncols + 15) & ~15;
+        const uint32_t id_pos = umma_idesc_mn(kT, n16, false), id_neg = umma_idesc_mn(kT, n16, true);
+        const int acc = j & 1, bb = j & 1;
+        if (!mbar_wait(&sh.acc_empty[acc], (uint32_t)(((j >> 1) & 1) ^ 1)) ||
+            !mbar_wait(&sh.b_full[bb], (uint32_t)((j >> 1) & 1))) {
+          fail(sh, status, w.p);
+          break;
+        }
+        const uint32_t re = tmem + (uint32_t)acc * (2 * kNS), im = re + kNS;
+        bool ok = true;
+        for (int s = 0; s < kSlabsS; ++s, ++g) {
+          const int ab = g % kAStages;
+          if (!mbar_wait(&sh.a_full[ab], (uint32_t)((g / kAStages) & 1))) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t sa = smem_u32(sh.a[ab]), sb = smem_u32(sh.b[bb]) + s * kSolveBSlab;
+          uint64_t A[4], Bv[4];
 #pragma unroll
-      for (int pl = 0; pl < 4; ++pl) {
-        A[pl] = umma_desc(sa + pl * kAPlane, alb, 128);
-        Bv[pl] = umma_desc(sb + pl * kBPlaneSlab, blb, 128);
+          for (int pl = 0; pl < 4; ++pl) {
+            A[pl] = umma_desc(sa + pl * kAPlane, alb, 128);
+            Bv[pl] = umma_desc(sb + pl * kSolveBPlaneSlab, blb, 128);
+          }
+          const uint32_t first = s == 0 ? 0u : 1u;
+          umma_bf16(re, A[0], Bv[0], id_pos, first);
+          umma_bf16(re, A[0], Bv[1], id_pos, 1);
+          umma_bf16(re, A[1], Bv[0], id_pos, 1);
+          umma_bf16(re, A[2], Bv[2], id_neg, 1);
+          umma_bf16(re, A[2], Bv[3], id_neg, 1);
+          umma_bf16(re, A[3], Bv[2], id_neg, 1);
+          umma_bf16(im, A[0], Bv[2], id_pos, first);
+          umma_bf16(im, A[0], Bv[3], id_pos, 1);
+          umma_bf16(im, A[1], Bv[2], id_pos, 1);
+          umma_bf16(im, A[2], Bv[0], id_pos, 1);
+          umma_bf16(im, A[2], Bv[1], id_pos, 1);
+          umma_bf16(im, A[3], Bv[0], id_pos, 1);
+          umma_commit(&sh.a_empty[ab]);
+        }
+        if (!ok) { fail(sh, status, w.p); break; }
+        umma_commit(&sh.acc_full[acc]);
+        umma_commit(&sh.b_empty[bb]);
       }
-      const uint32_t re = tmem, im = tmem + kNS;
-      const uint32_t first = s == 0 ? 0u : 1u;
-      umma_bf16(re, A[0], Bv[0], id_pos, first);
-      umma_bf16(re, A[0], Bv[1], id_pos, 1);
-      umma_bf16(re, A[1], Bv[0], id_pos, 1);
-      umma_bf16(re, A[2], Bv[2], id_neg, 1);
-      umma_bf16(re, A[2], Bv[3], id_neg, 1);
-      umma_bf16(re, A[3], Bv[2], id_neg, 1);
-      umma_bf16(im, A[0], Bv[2], id_pos, first);
-      umma_bf16(im, A[0], Bv[3], id_pos, 1);
-      umma_bf16(im, A[1], Bv[2], id_pos, 1);
-      umma_bf16(im, A[2], Bv[0], id_pos, 1);
-      umma_bf16(im, A[2], Bv[1], id_pos, 1);
-      umma_bf16(im, A[3], Bv[0], id_pos, 1);
-      umma_commit(&sh.done[buf]);
     }
-    issued = s + 1;
-  }
-  // wait for the MMAs of the last two committed slabs (bounded)
-  bool ok = true;
-  for (int s = issued - 2 < 0 ? 0 : issued - 2; s < issued; ++s)
-    ok = mbar_wait(&sh.done[s & 1], (uint32_t)((s >> 1) & 1)) && ok;
-  if (!ok || issued < kSlabsS) {
-    if (tid == 0) atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
-  } else {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // X_i rows 32 w + lane -= acc (columns [0, ncols) of the strip)
-    const int row = warp * 32 + lane;
-    const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
-    float2* xr = Xi + (size_t)row * nrhs + c0;
-    for (int c = 0; c < n16; c += 16) {
-      float vr[16], vi[16];
-      tmem_ld16(tmem + lane_addr + c, vr);
-      tmem_ld16(tmem + lane_addr + kNS + c, vi);
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        if (c + j < ncols) {
-          float2 v = xr[c + j];
-          v.x -= vr[j];
-          v.y -= vi[j];
-          xr[c + j] = v;
+  } else if (warp < kEpiWarp0) {
+    // ---------------------------------------------------------- converters
+    const int ct = threadIdx.x - kConvWarp0 * 32;  // 0 .. 127
+    int g = 0;
+    for (int it = blockIdx.x; it < total; it += work_ctas) {
+      bool ok = true;
+      for (int s = 0; s < kSlabsS; ++s, ++g) {
+        const int st = g % kRawStages, ab = g % kAStages;
+        const bool ready = mbar_wait(&sh.raw_full[st], (uint32_t)((g / kRawStages) & 1)) &&
+                           mbar_wait(&sh.a_empty[ab], (uint32_t)(((g / kAStages) & 1) ^ 1));
+        if (!__all_sync(0xffffffffu, ready ? 1 : 0) || sh.failed) {
+          ok = false;
+          break;
+        }
+        unsigned char* a = sh.a[ab];
+        const float* rre = sh.raw[st][0];
+        const float* rim = sh.raw[st][1];
+#pragma unroll 4
+        for (int e = ct; e < kT * (kSK / 2); e += kConvWarps * 32) {
+          int m, q;
+          float r0, r1, i0, i1;
+          if (OP == kOpPlain) {  // raw box [128 rows][16 cols]
+            m = e / (kSK / 2);
+            q = (e % (kSK / 2)) * 2;
+            const float2 rr = *reinterpret_cast<const float2*>(rre + m * kSK + q);
+            const float2 ii = *reinterpret_cast<const float2*>(rim + m * kSK + q);
+            r0 = rr.x; r1 = rr.y; i0 = ii.x; i1 = ii.y;
+          } else {  // raw box [16 rows][128 cols]
+            m = e % kT;
+            q = (e / kT) * 2;
+            r0 = rre[q * kT + m]; r1 = rre[(q + 1) * kT + m];
+            i0 = -rim[q * kT + m]; i1 = -rim[(q + 1) * kT + m];
+          }
+          __nv_bfloat162 rh, rl, ih, il;
+          split2(r0, r1, rh, rl);
+          split2(i0, i1, ih, il);
+          *reinterpret_cast<__nv_bfloat162*>(a + a_off(m, q, 0)) = rh;
+          *reinterpret_cast<__nv_bfloat162*>(a + a_off(m, q, 1)) = rl;
+          *reinterpret_cast<__nv_bfloat162*>(a + a_off(m, q, 2)) = ih;
+          *reinterpret_cast<__nv_bfloat162*>(a + a_off(m, q, 3)) = il;
+        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&sh.raw_empty[st]);
+          mbar_arrive(&sh.a_full[ab]);
         }
       }
+      if (!ok) {
+        if (lane == 0) fail(sh, status, item_of(it, n_items, strips).p);
+        break;
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int quarter = warp % 4;
+    const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+    const int row = quarter * 32 + lane;
+    int j = 0;
+    for (int it = blockIdx.x; it < total; it += work_ctas, ++j) {
+      const ItemOf w = item_of(it, n_items, strips);
+      const int acc = j & 1;
+      const bool ready = mbar_wait(&sh.acc_full[acc], (uint32_t)((j >> 1) & 1));
+      if (!__all_sync(0xffffffffu, ready ? 1 : 0)) {
+        if (lane == 0) fail(sh, status, w.p);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int c0 = w.strip * kNS;
+      const int ncols = nrhs - c0 < kNS ? nrhs - c0 : kNS;
+      const uint32_t base = tmem + (uint32_t)acc * (2 * kNS) + lane_addr;
+      float2* xr = work + ((size_t)w.p * n_pad + (size_t)tiles[w.tile_idx] * kT + row) * nrhs + c0;
+      float vr[2][16], vi[2][16];
+      tmem_ld16(base, vr[0]);
+      tmem_ld16(base + 16, vr[1]);
+      tmem_ld16(base + kNS, vi[0]);
+      tmem_ld16(base + kNS + 16, vi[1]);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh.acc_empty[acc]);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float2 xv[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+          xv[c] = h * 16 + c < ncols ? xr[h * 16 + c] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+          if (h * 16 + c < ncols)
+            xr[h * 16 + c] = make_float2(xv[c].x - vr[h][c], xv[c].y - vi[h][c]);
+      }
     }
   }
+  // Every role has left its loop (all waits are bounded).  A CTA that
+  // stopped early pauses (bounded, ~0.2 ms) so that its own TMA loads and
+  // MMAs still in flight land before the shared memory and TMEM go away.
+  __syncthreads();
+  if (sh.failed && threadIdx.x == 0)
+    for (int i = 0; i < 200; ++i) __nanosleep(1000);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
@@ -238,15 +344,16 @@ __global__ void __launch_bounds__(kSThreads) solve_tc_kernel(
 
 }  // namespace
 
-size_t solve_tc_smem() { return sizeof(SShared) + 1024; }
+size_t solve_tc_smem() { return sizeof(SShared) + 128; }
 
 // Launch the tensor-core update of step k for n tiles (device lists).
 int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, int op,
                     int np, int nrhs, const aosb_plan* P, const float* factor, float2* work,
-                    const float2* ytmp, int32_t* status, cudaStream_t st, char* err, size_t cap) {
+                    const float2* ytmp, const unsigned char* ystaged, int32_t* status,
+                    cudaStream_t st, char* err, size_t cap) {
   static bool attr_done[2] = {false, false};
   const size_t smem = solve_tc_smem();
-  static_assert(sizeof(SShared) + 1024 <= 232448, "shared memory budget");
+  static_assert(sizeof(SShared) + 128 <= 232448, "shared memory budget");
   if (!attr_done[op]) {
     cudaError_t e = op == kOpPlain
                         ? cudaFuncSetAttribute(solve_tc_kernel<kOpPlain>,
@@ -257,14 +364,29 @@ int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
       return set_error(err, cap, AOSB_ERR_CUDA, "solve_tc smem attribute: %s", cudaGetErrorString(e));
     attr_done[op] = true;
   }
+  // the factor as [rows][128] FP32; plain slabs are {16, 128} boxes,
+  // adjoint slabs {128, 16}
+  CUtensorMap fmap;
+  const uint64_t rows = (uint64_t)np * P->n_slots * 2 * kT;
+  if (int rc = op == kOpPlain
+                   ? encode_f32_2d((void*)factor, kT, rows, kSK, kT, false, &fmap, err, cap)
+                   : encode_f32_2d((void*)factor, kT, rows, kT, kSK, false, &fmap, err, cap))
+    return rc;
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const int strips = (nrhs + kNS - 1) / kNS;
-  dim3 g((unsigned)(n * strips + kCopyCtas), np);
+  const int64_t items = (int64_t)n * strips * np;
+  const int work_ctas = (int)(items < sms ? items : sms);
+  dim3 g((unsigned)(work_ctas + kCopyCtas));
   if (op == kOpPlain)
-    solve_tc_kernel<kOpPlain><<<g, kSThreads, smem, st>>>(k, n, nrhs, P->n_pad, dtiles, dslots,
-                                                          P->n_slots, factor, work, ytmp, status);
+    solve_tc_kernel<kOpPlain><<<g, kSThreads, smem, st>>>(k, n, nrhs, np, P->n_pad, dtiles, dslots,
+                                                          P->n_slots, work, ytmp, ystaged, status,
+                                                          fmap);
   else
-    solve_tc_kernel<kOpConjT><<<g, kSThreads, smem, st>>>(k, n, nrhs, P->n_pad, dtiles, dslots,
-                                                          P->n_slots, factor, work, ytmp, status);
+    solve_tc_kernel<kOpConjT><<<g, kSThreads, smem, st>>>(k, n, nrhs, np, P->n_pad, dtiles, dslots,
+                                                          P->n_slots, work, ytmp, ystaged, status,
+                                                          fmap);
   count_launches(1);
   return 0;
 }

@@ -8,9 +8,27 @@
 #include <cstdint>
 
 namespace aosb {
+
+// FP32 [rows][inner] tensor map with (box_x, box_y) boxes (tma_map.cu).
+int encode_f32_2d(void* base, uint64_t inner, uint64_t rows, uint32_t box_x, uint32_t box_y,
+                  bool swizzle128, CUtensorMap* map, char* err, size_t cap);
+
 namespace tc {
 
 constexpr long long kTcWaitLimit = 1ll << 22;  // polls (with backoff) before timeout
+
+// B operand of the tensor-core solve update: one 32-column RHS strip of a
+// step's diagonal result Y (K = 128 rows) as four BF16 planes (re_hi,
+// re_lo, im_hi, im_lo), K-major no-swizzle core matrices, 16-wide K slabs.
+constexpr int kSolveNS = 32;
+constexpr int kSolveBPlaneSlab = kSolveNS * 16 * 2;  // 1024 bytes
+constexpr int kSolveBSlab = 4 * kSolveBPlaneSlab;     // 4096 bytes
+constexpr int kSolveBBytes = 8 * kSolveBSlab;         // 32 KB per strip
+__host__ __device__ __forceinline__ uint32_t solve_b_offset(int n, int k, int plane) {
+  const int slab = k / 16, kk = k % 16;
+  return (uint32_t)(slab * kSolveBSlab + plane * kSolveBPlaneSlab + (kk / 8) * ((kSolveNS / 8) * 128) +
+                    (n / 8) * 128 + (n % 8) * 16 + (kk % 8) * 2);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -86,6 +104,16 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    smem_u32(bar))
                : "memory");
+}
+
+// smem tile = global box at (x, y); completion counted on `bar` (bytes).
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
 }
 
 // C[box at (x, y)] += smem tile (FP32 add in L2), one bulk group per commit.

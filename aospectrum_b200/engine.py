@@ -372,6 +372,7 @@ class BandEngine:
             self.plan = resources.plan
             self.row_blocks = resources.row_blocks
             self.pattern_seconds = self.analysis_seconds = 0.0
+            self.tuning = None
             if self.settings.search_dimension >= self.n:
                 raise SolverError("CISS search dimension must be smaller than matrix dimension")
             self._init_buffers()
@@ -398,9 +399,19 @@ class BandEngine:
         t0 = perf_counter()
         use_tc = self.engine.precision == "mixed" and self.engine.tensor_cores
         tile = self.engine.tile or (128 if use_tc else choose_tile(self.n))
-        self.plan = SymbolicPlan(self.n, self.pattern.indptr, self.pattern.indices, tile=tile,
-                                 supervariables=supervariables, ordering=self.engine.ordering,
-                                 device=self.device)
+        self.tuning = None
+        if self.engine.autotune and not self.engine.tile and self.bloch is not None:
+            from .autotune import tune_plan
+
+            h, s = self.bloch.apply(np.zeros((1, 3)))
+            self.plan, self.tuning = tune_plan(
+                self.n, self.pattern.indptr, self.pattern.indices, supervariables, h, s,
+                precision=self.precision_id(), device=self.device)
+            del h, s
+        else:
+            self.plan = SymbolicPlan(self.n, self.pattern.indptr, self.pattern.indices,
+                                     tile=tile, supervariables=supervariables,
+                                     ordering=self.engine.ordering, device=self.device)
         self.analysis_seconds = perf_counter() - t0
         self._init_buffers()
 
@@ -417,6 +428,13 @@ class BandEngine:
         self.factor_pencils: list[int] = []
 
     # ------------------------------------------------------------------ utils
+    def precision_id(self) -> int:
+        """The aosb_factor precision this engine's settings select."""
+        if self.engine.precision == "mixed" and self.engine.tensor_cores:
+            return (native.PRECISION_BF16X3 if self.engine.tensor_core_panels
+                    else native.PRECISION_BF16X3_FP32_PANELS)
+        return native.PRECISION_PLAIN
+
     def _stream(self):
         torch = _torch()
         return torch.cuda.current_stream(self.device).cuda_stream
@@ -465,6 +483,8 @@ class BandEngine:
         if self.engine.max_pencils:
             return self.engine.max_pencils
         free, _ = torch.cuda.mem_get_info(self.device)
+        # blocks the caching allocator holds but nobody uses are free for us
+        free += torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
         budget = int(free * self.engine.memory_fraction)
         return max(1, min(4096, budget // max(1, self.pencil_bytes(n_rhs))))
 
@@ -561,13 +581,12 @@ class BandEngine:
 
         work = pencil_schedule(nk, shifts, pair=mixed)
         cap = min(self.max_pencils(L), len(work))
+        # equal batches: 64 pencils under a cap of 48 run as 32 + 32, not 48 + 16
+        n_batches = -(-len(work) // cap)
+        cap = -(-len(work) // n_batches)
         info = self.plan.info
         lib = native.library()
-        if mixed and self.engine.tensor_cores:
-            precision = (native.PRECISION_BF16X3 if self.engine.tensor_core_panels
-                         else native.PRECISION_BF16X3_FP32_PANELS)
-        else:
-            precision = native.PRECISION_PLAIN
+        precision = self.precision_id()
         fbytes = lib.aosb_factor_bytes(self.plan.handle, cap)
         factor = torch.empty(fbytes // 4, dtype=torch.float32, device=dev)
         pivots = torch.empty((cap, info.n_pad), dtype=torch.int32, device=dev)
@@ -656,6 +675,8 @@ class BandEngine:
         mixed_tc = (self.engine.precision == "mixed" and self.engine.tensor_cores
                     and self.engine.tensor_core_solves and self.plan.info.tile == 128)
         flags = native.SOLVE_TENSOR_CORES if mixed_tc else 0
+        if self.engine.cuda_graphs:
+            flags |= native.SOLVE_GRAPH
         sa = native.SolveArgs(native.ABI_VERSION, native.C.sizeof(native.SolveArgs), np_, L,
                               adjoint, flags, factor.data_ptr(), pivots.data_ptr(), wn.data_ptr(),
                               self._solve_scratch.data_ptr(), st)
@@ -668,7 +689,7 @@ class BandEngine:
                         xn.data_ptr(), 1 if it > 0 else 0, st)
             if it < steps:
                 self._residual(n, L, np_, hvals, svals, pk, z, b, xn, rr, st)
-        if flags:
+        if flags & native.SOLVE_TENSOR_CORES:
             native.call("aosb_solve_check", self.plan.handle, native.C.byref(sa))
 
     residual_kernel = "blocks"   # "blocks" (rows of one atom share x loads) or "rows"

@@ -25,6 +25,7 @@ PRECISION_PLAIN = 0
 PRECISION_BF16X3 = 1
 PRECISION_BF16X3_FP32_PANELS = 2
 SOLVE_TENSOR_CORES = 1
+SOLVE_GRAPH = 2
 
 STATUS_NAMES = {
     10: "ABI mismatch", 11: "dimensions", 12: "batch", 13: "null pointer",

@@ -286,6 +286,12 @@ int aosb_factor(const aosb_plan_t *plan, const aosb_factor_args_v1 *args,
  * solves, aosb_solve_check synchronizes the stream and reports a timeout.
  * ------------------------------------------------------------------------ */
 #define AOSB_SOLVE_TENSOR_CORES 1
+/* AOSB_SOLVE_GRAPH: capture the solve's launch sequence into a CUDA graph
+ * the first time a (plan, n_pencils, n_rhs, adjoint, flags, factor, pivots,
+ * work, scratch) combination is seen and replay it afterwards; ignored while
+ * the stream is being captured by the caller.  Graphs are released with
+ * their plan. */
+#define AOSB_SOLVE_GRAPH 2
 
 typedef struct {
   uint32_t abi_version;

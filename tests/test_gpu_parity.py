@@ -379,3 +379,25 @@ def test_row_block_residual_matches_per_row(torch):
     finally:
         dev.close()
         plan.close()
+
+
+@pytest.mark.parametrize("adjoint", [0, 1])
+def test_graph_replayed_solve_equals_direct(adjoint, torch):
+    """AOSB_SOLVE_GRAPH: the first call captures, later calls replay; every
+    result equals the directly launched solve bit for bit."""
+    from aospectrum_b200 import native
+
+    b = bundles.small2d()
+    dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[1], torch, 64)
+    try:
+        rng = np.random.default_rng(4)
+        rhs = (rng.standard_normal((dev.n, 8)) + 1j * rng.standard_normal((dev.n, 8)))
+        shifts = [-2.3 + 0.01j, -2.0 + 0.2j]
+        ref = _factor_solve(dev, plan, h, s, shifts, rhs, torch, adjoint=adjoint, steps=1)
+        for _ in range(3):
+            got = _factor_solve(dev, plan, h, s, shifts, rhs, torch, adjoint=adjoint, steps=1,
+                                flags=native.SOLVE_GRAPH)
+            assert np.array_equal(got, ref)
+    finally:
+        dev.close()
+        plan.close()
