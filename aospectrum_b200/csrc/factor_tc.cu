@@ -30,6 +30,7 @@
 #include "factor.h"
 #include "cgemm.cuh"
 #include "tc_common.cuh"
+#include "timing.h"
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -39,22 +40,6 @@
 #include <vector>
 
 namespace aosb {
-
-// Optional CUDA-event timing of every schur_tc_kernel launch (on the stream
-// the kernel is launched on), with its algorithmic work: 8 T^3 real flops
-// per (target tile, pencil) and 256 KB of target read + write per target
-// plus one read of each staged operand tile.
-struct SchurTimer {
-  std::mutex mu;
-  bool on = false;
-  std::vector<cudaEvent_t> events;  // start, stop pairs
-  double flops = 0.0, bytes = 0.0;
-  int64_t launches = 0;
-};
-SchurTimer& schur_timer() {
-  static SchurTimer t;
-  return t;
-}
 
 namespace {
 
@@ -615,31 +600,16 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     const int nL = P->lb_off[k + 1] - P->lb_off[k];
     const int nU = P->ur_off[k + 1] - P->ur_off[k];
     const int64_t items = (int64_t)n_pairs * np;
-    SchurTimer& tm = schur_timer();
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-    {
-      std::lock_guard<std::mutex> lock(tm.mu);
-      if (tm.on && cudaEventCreate(&ev[0]) == cudaSuccess && cudaEventCreate(&ev[1]) == cudaSuccess) {
-        cudaEventRecord(ev[0], st);
-      } else {
-        if (ev[0]) cudaEventDestroy(ev[0]);
-        ev[0] = ev[1] = nullptr;
-      }
-    }
+    cudaEvent_t ev[2];
+    const bool timed = timing_begin(st, ev);
     const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr};
     schur_tc_kernel<<<grid_for(items, cap_ctas), kPThreads, smem, st>>>(
         sm, np, P->n_slots, stage_buf(k), pencil_stride, a->status, tmap_c);
     count_launches(1);
-    if (ev[0] != nullptr) {
-      cudaEventRecord(ev[1], st);
-      std::lock_guard<std::mutex> lock(tm.mu);
-      tm.events.push_back(ev[0]);
-      tm.events.push_back(ev[1]);
-      tm.flops += (double)items * 8.0 * kTcT * kTcT * kTcT;
-      tm.bytes += (double)items * 2.0 * 2 * kTcT * kTcT * sizeof(float) +
-                  (double)(nL + nU) * np * kStagedTileBytes * ((double)n_pairs / (nL * nU));
-      tm.launches += 1;
-    }
+    if (timed)
+      timing_end(kTimedSchur, st, ev, (double)items * 8.0 * kTcT * kTcT * kTcT,
+                 (double)items * 2.0 * 2 * kTcT * kTcT * sizeof(float) +
+                     (double)(nL + nU) * np * kStagedTileBytes * ((double)n_pairs / (nL * nU)));
   };
 
   for (int64_t k = 0; k < P->nb; ++k) {
@@ -690,34 +660,3 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
 }
 
 }  // namespace aosb
-
-extern "C" int aosb_kernel_timing(int32_t enable) {
-  aosb::SchurTimer& t = aosb::schur_timer();
-  std::lock_guard<std::mutex> lock(t.mu);
-  for (cudaEvent_t e : t.events) cudaEventDestroy(e);
-  t.events.clear();
-  t.flops = t.bytes = 0.0;
-  t.launches = 0;
-  t.on = enable != 0;
-  return 0;
-}
-
-extern "C" int aosb_kernel_timing_read(double* total_ms, double* flops, double* bytes,
-                                       int64_t* launches) {
-  aosb::SchurTimer& t = aosb::schur_timer();
-  std::lock_guard<std::mutex> lock(t.mu);
-  double ms = 0.0;
-  for (size_t i = 0; i + 1 < t.events.size(); i += 2) {
-    if (cudaEventSynchronize(t.events[i + 1]) != cudaSuccess) return AOSB_ERR_CUDA;
-    float one = 0.0f;
-    if (cudaEventElapsedTime(&one, t.events[i], t.events[i + 1]) != cudaSuccess)
-      return AOSB_ERR_CUDA;
-    ms += one;
-  }
-  if (total_ms) *total_ms = ms;
-  if (flops) *flops = t.flops;
-  if (bytes) *bytes = t.bytes;
-  if (launches) *launches = t.launches;
-  return 0;
-}
-

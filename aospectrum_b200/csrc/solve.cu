@@ -15,6 +15,7 @@
 #include "plan.h"
 #include "cgemm.cuh"
 #include "tc_common.cuh"
+#include "timing.h"
 
 #include <cuda_bf16.h>
 
@@ -203,22 +204,35 @@ int run_solve(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t
   auto diag = [&](int k, int op) {
     count_launches(1);
     dim3 g(ncs, T / 32, np);
+    cudaEvent_t ev[2];
+    const bool timed = timing_begin(st, ev);
     switch (op) {
       case kLinv: solve_diag_kernel<T, kLinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
       case kUinv: solve_diag_kernel<T, kUinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
       case kUinvH: solve_diag_kernel<T, kUinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
       default: solve_diag_kernel<T, kLinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
     }
+    // algorithmic: one triangular T x T tile times T x L per pencil
+    if (timed)
+      timing_end(kTimedSolveDiag, st, ev, 4.0 * T * T * L * np,
+                 (double)np * (2.0 * T * T * sizeof(float) + 2.0 * T * L * sizeof(float2)));
   };
   if (tc) AOSB_CUDA_TRY(cudaMemsetAsync(tc_status, 0, (size_t)np * sizeof(int32_t), st), err, cap);
   int tc_rc = 0;
   auto update = [&](int k, const std::vector<int32_t>& off, const int32_t* dtiles,
                     const int32_t* dslots, int op) {
     const int n = off[k + 1] - off[k];
+    cudaEvent_t ev[2];
+    const bool timed = timing_begin(st, ev);
+    // algorithmic: n tiles x (T x T) x (T x L) complex per pencil; factor
+    // tiles read once, X tiles read and written
+    const double uflops = 8.0 * T * T * L * (double)n * np;
+    const double ubytes = (double)n * np * (2.0 * T * T * sizeof(float) + 2.0 * T * L * sizeof(float2));
     if (tc) {
       if (tc_rc == 0)
         tc_rc = solve_tc_update(k, n, dtiles + off[k], dslots + off[k], op, np, L, P, a->factor,
                                 W, Y, ystaged, tc_status, st, err, cap);
+      if (timed) timing_end(kTimedSolveUpdate, st, ev, uflops, ubytes);
       return;
     }
     dim3 g((unsigned)(n * rowblocks * ncs + kCopyBlocks), np);
@@ -227,6 +241,7 @@ int run_solve(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t
       solve_update_kernel<T, kPlain><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + off[k], dslots + off[k], P->n_slots, a->factor, W, Y);
     else
       solve_update_kernel<T, kConjT><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + off[k], dslots + off[k], P->n_slots, a->factor, W, Y);
+    if (timed) timing_end(kTimedSolveUpdate, st, ev, uflops, ubytes);
   };
   const int nb = (int)P->nb;
   if (!a->adjoint) {

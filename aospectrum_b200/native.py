@@ -98,6 +98,9 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_kernel_timing": (C.c_int, [c_i32]),
     "aosb_kernel_timing_read": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double),
                                           C.POINTER(C.c_double), C.POINTER(c_i64)]),
+    "aosb_kernel_timing_read_category": (C.c_int, [c_i32, C.POINTER(C.c_double),
+                                                   C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                                   C.POINTER(c_i64)]),
     "aospectrum_b200_solve_complex64_ubatch_v1": (C.c_int, [C.POINTER(UbatchRequest),
                                                             C.POINTER(UbatchResult)]),
     "aosb_bloch_create": (C.c_int, [c_i64, c_i64, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp,

@@ -59,6 +59,8 @@ def parse() -> argparse.Namespace:
                     help="FP64 refinement sweeps per mixed solve (-1 = engine default)")
     ap.add_argument("--max-pencils", type=int, default=0,
                     help="cap on pencils factored together (0 = by memory)")
+    ap.add_argument("--ordering", choices=("auto", "natural", "nested_dissection"),
+                    default="auto", help="tile-plan ordering when not autotuned")
     ap.add_argument("--autotune", type=int, default=1,
                     help="1: time candidate tile plans and k-point batches on the device first")
     ap.add_argument("--tensor-core-solves", type=int, default=-1,
@@ -225,6 +227,7 @@ def main() -> None:
                      EngineSettings(precision=args.precision,
                                     tensor_cores=bool(args.tensor_cores),
                                     autotune=bool(args.autotune),
+                                    ordering=args.ordering,
                                     max_pencils=args.max_pencils,
                                     **({"refinement_steps": args.refinement_steps}
                                        if args.refinement_steps >= 0 else {}),
@@ -287,6 +290,20 @@ def main() -> None:
                                           native.C.c_double(), native.c_i64())
     native.library().aosb_kernel_timing_read(native.C.byref(k_ms), native.C.byref(k_flops),
                                              native.C.byref(k_bytes), native.C.byref(k_launches))
+    breakdown = {}
+    for cat, name in ((1, "solve_diag"), (2, "solve_update")):
+        c_ms, c_fl, c_by, c_n = (native.C.c_double(), native.C.c_double(), native.C.c_double(),
+                                 native.c_i64())
+        native.library().aosb_kernel_timing_read_category(
+            cat, native.C.byref(c_ms), native.C.byref(c_fl), native.C.byref(c_by),
+            native.C.byref(c_n))
+        if c_n.value:
+            breakdown[name] = {"ms_per_step": c_ms.value / args.steps, "launches": int(c_n.value),
+                               "avg_launch_us": 1e3 * c_ms.value / c_n.value,
+                               "gbs": c_by.value / (c_ms.value / 1e3) / 1e9,
+                               "tflops": c_fl.value / (c_ms.value / 1e3) / 1e12}
+    breakdown["schur_tc"] = {"ms_per_step": k_ms.value / args.steps,
+                             "launches": int(k_launches.value)}
     native.library().aosb_kernel_timing(0)
     t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
     if world > 1:
@@ -357,9 +374,15 @@ def main() -> None:
                        info.factor_bytes / 1e9),
                    "parallelism": f"dp{world} (k points sharded)"},
         "gpu_launches": int(launches),
+        "kernel_event_times": breakdown,
         "clocks": clocks.summary(),
         "roofline": roofline,
     }
+    total_mem = torch.cuda.get_device_properties(dev).total_memory
+    out["memory"] = {"peak_allocated_gb": torch.cuda.max_memory_allocated(dev) / 1e9,
+                     "factor_gb_per_pencil": info.factor_bytes / 1e9,
+                     "factor_gb_resident": info.factor_bytes * stats.get("pencil_batch", 1) / 1e9,
+                     "device_total_gb": total_mem / 1e9}
     if rank == 0:
         out["stage_seconds_last_step"] = {k: round(v, 4) for k, v in
                                           stats.get("stage_seconds", {}).items()}
