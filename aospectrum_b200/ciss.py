@@ -109,7 +109,7 @@ class EngineSettings:
     ordering: str = "auto"
     tensor_cores: bool = True
     tensor_core_panels: bool = True
-    tensor_core_solves: bool = False
+    tensor_core_solves: bool = True
     autotune: bool = False
     cuda_graphs: bool = False
 

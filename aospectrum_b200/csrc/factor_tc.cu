@@ -615,8 +615,9 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   for (int64_t k = 0; k < P->nb; ++k) {
     const int nL = P->lb_off[k + 1] - P->lb_off[k];
     const int nU = P->ur_off[k + 1] - P->ur_off[k];
-    if ((int64_t)nL * nU > INT32_MAX / 65536)
-      return set_error(err, cap, AOSB_ERR_SIZE, "too many Schur targets in one step");
+    // the kernel enumerates (target, pencil) items in 32-bit ints
+    if ((int64_t)nL * nU * np > INT32_MAX)
+      return set_error(err, cap, AOSB_ERR_SIZE, "too many Schur targets x pencils in one step");
     if (!tc_panels) {
       if (int rc = factor_step_panels(P, a, (int)k, err, cap)) return rc;
       stage_schur(k, st);

@@ -20,7 +20,9 @@
 //                   accumulator pairs (re, im): hi*hi + hi*lo + lo*hi per real
 //                   product, FP32 accumulation;
 //   warps 6-9       epilogue: tcgen05.ld of the accumulator (warp w reads
-//                   lanes 32 (w % 4) ..), X_i -= acc.
+//                   lanes 32 (w % 4) ..); -acc goes through 128B-swizzled
+//                   shared boxes into TMA reduce-adds on X_i (coalesced and
+//                   asynchronous: X never passes through the registers).
 // Two accumulator pairs let one item's epilogue overlap the next item's
 // MMAs.  Every mbarrier wait is bounded: on expiry the CTA records
 // AOSB_ERR_TIMEOUT in the pencil status and stops; a CTA that stops waits
@@ -54,6 +56,10 @@ constexpr int kCopyCtas = 4;
 enum SolveOp { kOpPlain = 0, kOpConjT = 1 };
 
 struct SShared {
+  // per epilogue warp: its 32 rows x 32 complex of -acc as two 32 x 32 FP32
+  // boxes (complex columns 0-15 and 16-31, re/im interleaved), laid out as
+  // the TMA 128-byte swizzle expects
+  alignas(1024) float ep[kEpiWarps][2][32 * 32];       // 32 KB
   alignas(128) float raw[kRawStages][2][kRawPlane];   // 64 KB
   alignas(128) unsigned char a[kAStages][kASlab];      // 48 KB
   alignas(128) unsigned char b[2][kSolveBBytes];       // 64 KB
@@ -103,7 +109,8 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
     int k, int n_items, int nrhs, int n_pencils, int64_t n_pad, const int32_t* __restrict__ tiles,
     const int32_t* __restrict__ slots, int64_t n_slots, float2* __restrict__ work,
     const float2* __restrict__ ytmp, const unsigned char* __restrict__ ystaged,
-    int32_t* __restrict__ status, const __grid_constant__ CUtensorMap fmap) {
+    int32_t* __restrict__ status, const __grid_constant__ CUtensorMap fmap,
+    const __grid_constant__ CUtensorMap xmap, int x_tma) {
   const int strips = (nrhs + kNS - 1) / kNS;
   const int total = n_items * strips * n_pencils;
   const int work_ctas = (int)gridDim.x - kCopyCtas;
@@ -120,7 +127,7 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
   }
   extern __shared__ unsigned char dyn[];
   SShared& sh = *reinterpret_cast<SShared*>(
-      (reinterpret_cast<uintptr_t>(dyn) + 127) & ~(uintptr_t)127);
+      (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kRawStages; ++s) {
@@ -290,9 +297,15 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
     }
   } else {
     // ------------------------------------------------------------ epilogue
+    // X rows of an item are contiguous (n_rhs complex each).  With x_tma the
+    // warp writes -acc for its 32 rows into its swizzled boxes and lane 0
+    // hands them to TMA reduce-adds into X in L2 (coalesced, asynchronous);
+    // otherwise every lane read-modify-writes its row.
     const int quarter = warp % 4;
+    const int ew = warp - kEpiWarp0;
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
     const int row = quarter * 32 + lane;
+    const int sw = lane & 7;
     int j = 0;
     for (int it = blockIdx.x; it < total; it += work_ctas, ++j) {
       const ItemOf w = item_of(it, n_items, strips);
@@ -306,7 +319,6 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
       const int c0 = w.strip * kNS;
       const int ncols = nrhs - c0 < kNS ? nrhs - c0 : kNS;
       const uint32_t base = tmem + (uint32_t)acc * (2 * kNS) + lane_addr;
-      float2* xr = work + ((size_t)w.p * n_pad + (size_t)tiles[w.tile_idx] * kT + row) * nrhs + c0;
       float vr[2][16], vi[2][16];
       tmem_ld16(base, vr[0]);
       tmem_ld16(base + 16, vr[1]);
@@ -315,18 +327,45 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh.acc_empty[acc]);
+      const int64_t xrow = (int64_t)w.p * n_pad + (int64_t)tiles[w.tile_idx] * kT;
+      if (x_tma) {
+        if (lane == 0) bulk_wait_read_all();   // the boxes' previous reduce has read them
+        __syncwarp();
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        float2 xv[16];
+        for (int h = 0; h < 2; ++h) {
+          float* box = sh.ep[ew][h];
+          // 16 complex = 32 floats = 8 chunks of 16 bytes: (re, im, re, im)
 #pragma unroll
-        for (int c = 0; c < 16; ++c)
-          xv[c] = h * 16 + c < ncols ? xr[h * 16 + c] : make_float2(0.f, 0.f);
+          for (int c = 0; c < 8; ++c)
+            *reinterpret_cast<float4*>(box + lane * 32 + ((c ^ sw) * 4)) =
+                make_float4(-vr[h][2 * c], -vi[h][2 * c], -vr[h][2 * c + 1], -vi[h][2 * c + 1]);
+        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          const int y = (int)(xrow + quarter * 32);
+          tma_reduce_add_2d(&xmap, sh.ep[ew][0], 2 * c0, y);
+          if (ncols > 16) tma_reduce_add_2d(&xmap, sh.ep[ew][1], 2 * c0 + 32, y);
+          bulk_commit();
+        }
+      } else {
+        float2* xr = work + (size_t)(xrow + row) * nrhs + c0;
 #pragma unroll
-        for (int c = 0; c < 16; ++c)
-          if (h * 16 + c < ncols)
-            xr[h * 16 + c] = make_float2(xv[c].x - vr[h][c], xv[c].y - vi[h][c]);
+        for (int h = 0; h < 2; ++h) {
+          float2 xv[16];
+#pragma unroll
+          for (int c = 0; c < 16; ++c)
+            xv[c] = h * 16 + c < ncols ? xr[h * 16 + c] : make_float2(0.f, 0.f);
+#pragma unroll
+          for (int c = 0; c < 16; ++c)
+            if (h * 16 + c < ncols)
+              xr[h * 16 + c] = make_float2(xv[c].x - vr[h][c], xv[c].y - vi[h][c]);
+        }
       }
     }
+    // the X updates must be complete (not only read) before exit
+    if (x_tma && lane == 0) bulk_wait_all();
+    __syncwarp();
   }
   // Every role has left its loop (all waits are bounded).  A CTA that
   // stopped early pauses (bounded, ~0.2 ms) so that its own TMA loads and
@@ -344,7 +383,7 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
 
 }  // namespace
 
-size_t solve_tc_smem() { return sizeof(SShared) + 128; }
+size_t solve_tc_smem() { return sizeof(SShared) + 1024; }
 
 // Launch the tensor-core update of step k for n tiles (device lists).
 int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, int op,
@@ -353,7 +392,7 @@ int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
                     cudaStream_t st, char* err, size_t cap) {
   static bool attr_done[2] = {false, false};
   const size_t smem = solve_tc_smem();
-  static_assert(sizeof(SShared) + 128 <= 232448, "shared memory budget");
+  static_assert(sizeof(SShared) + 1024 <= 232448, "shared memory budget");
   if (!attr_done[op]) {
     cudaError_t e = op == kOpPlain
                         ? cudaFuncSetAttribute(solve_tc_kernel<kOpPlain>,
@@ -372,6 +411,18 @@ int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
                    ? encode_f32_2d((void*)factor, kT, rows, kSK, kT, false, &fmap, err, cap)
                    : encode_f32_2d((void*)factor, kT, rows, kT, kSK, false, &fmap, err, cap))
     return rc;
+  // X as [n_pencils * n_pad rows][2 n_rhs] FP32, 32 x 32 boxes, 128-byte
+  // swizzle: the destination of the epilogue's reduce-adds (rows of 2 n_rhs
+  // floats must be a multiple of 16 bytes: n_rhs even)
+  CUtensorMap xmap;
+  const int x_tma = (nrhs % 2 == 0) ? 1 : 0;
+  if (x_tma) {
+    if (int rc = encode_f32_2d((void*)work, (uint64_t)2 * nrhs, (uint64_t)np * P->n_pad, 32, 32,
+                               true, &xmap, err, cap))
+      return rc;
+  } else {
+    xmap = fmap;  // unused
+  }
   int device = 0, sms = 148;
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -382,11 +433,11 @@ int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
   if (op == kOpPlain)
     solve_tc_kernel<kOpPlain><<<g, kSThreads, smem, st>>>(k, n, nrhs, np, P->n_pad, dtiles, dslots,
                                                           P->n_slots, work, ytmp, ystaged, status,
-                                                          fmap);
+                                                          fmap, xmap, x_tma);
   else
     solve_tc_kernel<kOpConjT><<<g, kSThreads, smem, st>>>(k, n, nrhs, np, P->n_pad, dtiles, dslots,
                                                           P->n_slots, work, ytmp, ystaged, status,
-                                                          fmap);
+                                                          fmap, xmap, x_tma);
   count_launches(1);
   return 0;
 }

@@ -57,7 +57,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
-    if (it > 64) __nanosleep(128);
+    if (it > 4096) __nanosleep(64);   // spin first: pipeline handoffs are sub-microsecond
   }
   return false;
 }

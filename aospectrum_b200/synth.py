@@ -301,3 +301,39 @@ def small_spec(name: str = "tiny", side: int = 3, orbitals: int = 5, seed: int =
                              periodic=(True, True, False), cutoff=4.0,
                              orbitals_per_atom=orbitals, seed=seed, origin=(0, 0, 7.5))
     return replace(_cubic(name, side, 2.4, 4.0), orbitals_per_atom=orbitals, seed=seed)
+
+
+@dataclass(frozen=True)
+class ServingRequestSpec:
+    """One request of a seeded serving stream."""
+
+    spec: SyntheticSpec
+    kpoint_indices: tuple[int, ...]   # indices into the Y-G-X-M path
+    states: int                        # states the window holds at Gamma
+    arrival_s: float                   # offset from the start of the stream
+
+
+def serving_stream(n_requests: int = 12, *, seed: int = 20261203, rate_per_s: float = 2.0,
+                   sides: tuple[int, ...] = (6, 7, 8, 9, 10),
+                   kpoints: tuple[int, int] = (4, 16), states: tuple[int, int] = (20, 60)
+                   ) -> list[ServingRequestSpec]:
+    """A seeded stream of band requests for the serving benchmark: cubic
+    bundles of side**3 atoms (216-1000 with the default sides) with 13
+    (Ti-like) or 5 (C-like) orbitals per atom, k points drawn from the
+    121-point Y-G-X-M path, windows holding ``states`` Gamma states, and
+    Poisson arrivals at ``rate_per_s``.  Bundles repeat across requests
+    (same side, orbitals and seed), as a service sees repeated systems."""
+    rng = np.random.default_rng(seed)
+    out = []
+    t = 0.0
+    for _ in range(n_requests):
+        side = int(rng.choice(sides))
+        orbitals = int(rng.choice([13, 5]))
+        spec = replace(_cubic(f"serve-{side}-{orbitals}", side, 2.4, 7.0),
+                       orbitals_per_atom=orbitals, seed=1000 + side * 17 + orbitals)
+        nk = int(rng.integers(kpoints[0], kpoints[1] + 1))
+        ks = tuple(int(v) for v in np.sort(rng.choice(121, size=nk, replace=False)))
+        st = int(rng.integers(states[0], states[1] + 1))
+        out.append(ServingRequestSpec(spec, ks, st, t))
+        t += float(rng.exponential(1.0 / rate_per_s))
+    return out
