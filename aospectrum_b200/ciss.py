@@ -94,6 +94,9 @@ class EngineSettings:
     tensor_core_solves: with tensor cores, run the off-diagonal tile
         updates of the triangular sweeps in split BF16 too (FP64
         refinement recovers the accuracy); False keeps them in FP32 SIMT.
+    schur_depth: 2 applies the Schur updates of two tile steps in one
+        tensor-core pass (K = 256: each target tile read and written once per
+        two steps); 1 updates after every step.
     cuda_graphs: capture each batch's triangular sweeps (hundreds of
         launches per solve) into a CUDA graph on first use and replay it.
     autotune: with tile 0, time the candidate tile plans (tile edge x
@@ -111,6 +114,7 @@ class EngineSettings:
     tensor_core_panels: bool = True
     tensor_core_solves: bool = True
     autotune: bool = False
+    schur_depth: int = 1
     cuda_graphs: bool = False
 
     def __post_init__(self) -> None:
@@ -122,6 +126,8 @@ class EngineSettings:
             raise InputError("refinement_steps and max_pencils must be >= 0")
         if not 0.0 < self.memory_fraction <= 0.95:
             raise InputError("memory_fraction must be in (0, 0.95]")
+        if self.schur_depth not in (1, 2):
+            raise InputError("schur_depth must be 1 or 2")
         if self.ordering not in ("auto", "nested_dissection", "natural"):
             raise InputError("ordering must be auto, nested_dissection or natural")
 

@@ -336,7 +336,8 @@ int aospectrum_b200_solve_complex64_ubatch_v1(const aospectrum_b200_ubatch_reque
 extern "C" size_t aosb_factor_workspace_bytes(const aosb_plan_t* plan, int32_t n_pencils,
                                               int32_t precision) {
   if (plan == nullptr || n_pencils <= 0) return 0;
-  if (precision == AOSB_PRECISION_BF16X3 || precision == AOSB_PRECISION_BF16X3_FP32_PANELS)
+  if (precision == AOSB_PRECISION_BF16X3 || precision == AOSB_PRECISION_BF16X3_FP32_PANELS ||
+      precision == AOSB_PRECISION_BF16X3_ONE_STEP)
     return aosb::factor_tc_workspace(plan, n_pencils);
   return 0;
 }

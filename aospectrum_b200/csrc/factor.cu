@@ -610,7 +610,8 @@ int aosb_factor(const aosb_plan_t* plan, const aosb_factor_args_v1* a, char* err
   int rc = aosb::factor_assemble(plan, a, err, cap);
   if (rc) return rc;
   if (a->precision == AOSB_PRECISION_PLAIN) return aosb::factor_plain(plan, a, err, cap);
-  if (a->precision == AOSB_PRECISION_BF16X3 || a->precision == AOSB_PRECISION_BF16X3_FP32_PANELS)
+  if (a->precision == AOSB_PRECISION_BF16X3 || a->precision == AOSB_PRECISION_BF16X3_FP32_PANELS ||
+      a->precision == AOSB_PRECISION_BF16X3_ONE_STEP)
     return aosb::factor_tc(plan, a, err, cap);
   return set_error(err, cap, AOSB_ERR_ARGUMENT, "unknown precision %d", a->precision);
 }

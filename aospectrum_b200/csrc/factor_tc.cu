@@ -208,14 +208,24 @@ struct PShared {
 //     k + 1, "cross" holds the pairs with a < a0 or b < b0 -- every target
 //     in tile row or column k + 1, which step k + 1's diagonal LU and panels
 //     read -- and "rest" the pairs with a >= a0 and b >= b0.
-enum MapKind : int { kMapSchur = 0, kMapPanel = 1, kMapCross = 2, kMapRest = 3 };
+//   kMapList: two-step (K = 256) Schur items from the plan's super-step
+//     lists: item = (target slot, A and B staged index of the first step or
+//     -1, of the second step or -1); the first step's tiles come from
+//     `staging`, the second's from `staging1`.
+enum MapKind : int { kMapSchur = 0, kMapPanel = 1, kMapCross = 2, kMapRest = 3, kMapList = 4 };
 
 struct ItemMap {
   int kind, nL, nU, n_pairs, a0, b0;
   const int32_t* tslot;  // Schur targets [nL * nU]
   const int32_t* lslot;  // panel L targets [nL]
   const int32_t* uslot;  // panel U targets [nU]
+  const int32_t* list;   // kMapList items [n_pairs][5]
 };
+
+// K halves of an item: staged (A, B) indices and which staging buffer
+// (0 = `staging`, 1 = `staging1`); returns how many (1 or 2).
+__device__ __forceinline__ int item_halves(const ItemMap& m, int pair, int (&ia)[2], int (&ib)[2],
+                                           int (&buf)[2]);
 
 __device__ __forceinline__ void item_pair(const ItemMap& m, int pair, int& a, int& b) {
   if (m.kind == kMapSchur) {
@@ -255,7 +265,32 @@ __device__ __forceinline__ void item_operands(const ItemMap& m, int pair, int& i
   ib = m.nL + b;
 }
 
+__device__ __forceinline__ int item_halves(const ItemMap& m, int pair, int (&ia)[2], int (&ib)[2],
+                                           int (&buf)[2]) {
+  if (m.kind != kMapList) {
+    item_operands(m, pair, ia[0], ib[0]);
+    buf[0] = 0;
+    return 1;
+  }
+  const int32_t* e = m.list + (size_t)pair * 5;
+  int nh = 0;
+  if (e[1] >= 0) {
+    ia[nh] = e[1];
+    ib[nh] = e[2];
+    buf[nh] = 0;
+    ++nh;
+  }
+  if (e[3] >= 0) {
+    ia[nh] = e[3];
+    ib[nh] = e[4];
+    buf[nh] = 1;
+    ++nh;
+  }
+  return nh;
+}
+
 __device__ __forceinline__ int item_target(const ItemMap& m, int pair) {
+  if (m.kind == kMapList) return m.list[(size_t)pair * 5];
   if (m.kind == kMapPanel) return pair < m.nL ? m.lslot[pair] : m.uslot[pair - m.nL];
   int a, b;
   item_pair(m, pair, a, b);
@@ -264,8 +299,8 @@ __device__ __forceinline__ int item_target(const ItemMap& m, int pair) {
 
 __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     const ItemMap map, int n_pencils, int64_t n_slots, const unsigned char* __restrict__ staging,
-    int64_t staging_pencil_stride, int32_t* __restrict__ status,
-    const __grid_constant__ CUtensorMap tmap_c) {
+    const unsigned char* __restrict__ staging1, int64_t staging_pencil_stride,
+    int32_t* __restrict__ status, const __grid_constant__ CUtensorMap tmap_c) {
   const int n_pairs = map.n_pairs;
   extern __shared__ unsigned char dyn[];
   PShared& sh = *reinterpret_cast<PShared*>(
@@ -301,22 +336,22 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
       uint32_t phase = 0;
       for (int it = blockIdx.x; it < total && !sh.failed; it += gridDim.x) {
         const int p = it / n_pairs, pair = it % n_pairs;
-        int ia, ib;
-        item_operands(map, pair, ia, ib);
-        const unsigned char* stA = staging + (size_t)p * staging_pencil_stride +
-                                   (size_t)ia * kStagedTileBytes;
-        const unsigned char* stB = staging + (size_t)p * staging_pencil_stride +
-                                   (size_t)ib * kStagedTileBytes;
-        for (int s = 0; s < kSlabs; ++s) {
+        int ia[2], ib[2], bf[2];
+        const int nh = item_halves(map, pair, ia, ib, bf);
+        for (int s = 0; s < nh * kSlabs; ++s) {
+          const int h = s / kSlabs, sl = s % kSlabs;
+          const unsigned char* base = (bf[h] ? staging1 : staging) + (size_t)p * staging_pencil_stride;
+          const unsigned char* stA = base + (size_t)ia[h] * kStagedTileBytes;
+          const unsigned char* stB = base + (size_t)ib[h] * kStagedTileBytes;
           if (!mbar_wait(&sh.empty[stage], phase ^ 1)) {
             sh.failed = 1;
             atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
             break;
           }
           mbar_expect_tx(&sh.full[stage], 2 * kOperandSlabBytes);
-          bulk_g2s(sh.a[stage], stA + (size_t)s * kOperandSlabBytes, kOperandSlabBytes,
+          bulk_g2s(sh.a[stage], stA + (size_t)sl * kOperandSlabBytes, kOperandSlabBytes,
                    &sh.full[stage]);
-          bulk_g2s(sh.b[stage], stB + (size_t)s * kOperandSlabBytes, kOperandSlabBytes,
+          bulk_g2s(sh.b[stage], stB + (size_t)sl * kOperandSlabBytes, kOperandSlabBytes,
                    &sh.full[stage]);
           if (++stage == kStagesP) { stage = 0; phase ^= 1; }
         }
@@ -330,6 +365,8 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
       uint32_t phase = 0, acc_phase = 0;
       for (int it = blockIdx.x; it < total && !sh.failed; it += gridDim.x) {
         const int p = it / n_pairs;
+        int ia[2], ib[2], bf[2];
+        const int nslabs = item_halves(map, it % n_pairs, ia, ib, bf) * kSlabs;
         if (!mbar_wait(&sh.acc_empty[acc], acc_phase ^ 1)) {
           sh.failed = 1;
           atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
@@ -338,7 +375,7 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t re = tmem + (uint32_t)acc * 256, im = re + kTcT;
         bool ok = true;
-        for (int s = 0; s < kSlabs; ++s) {
+        for (int s = 0; s < nslabs; ++s) {
           if (!mbar_wait(&sh.full[stage], phase)) {
             ok = false;
             break;
@@ -471,11 +508,12 @@ static int64_t staged_tiles_per_pencil(const aosb_plan* P) {
   return most + 2;
 }
 
-// Two staging buffers: with lookahead, step k + 1's panels are staged while
-// step k's Schur update still reads step k's tiles.
+// Four staging buffers (tile step k uses buffer k % 4): with two-step
+// updates and lookahead, steps k + 2 and k + 3 are staged while the
+// two-step update of steps k and k + 1 still reads theirs.
 size_t factor_tc_workspace(const aosb_plan* P, int32_t n_pencils) {
   if (P->T != kTcT) return 0;
-  return 2 * (size_t)staged_tiles_per_pencil(P) * kStagedTileBytes * (size_t)n_pencils;
+  return 4 * (size_t)staged_tiles_per_pencil(P) * kStagedTileBytes * (size_t)n_pencils;
 }
 
 // Side stream of a caller stream for the lookahead panels (created once,
@@ -564,7 +602,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     }
   } guard{ev_cross, ev_panel};
   const int64_t buffer_bytes = (int64_t)np * pencil_stride;
-  auto stage_buf = [&](int64_t k) { return staging + (k & 1) * buffer_bytes; };
+  auto stage_buf = [&](int64_t k) { return staging + (k & 3) * buffer_bytes; };
 
   // diagonal LU + panel products of step k on stream s (panel grid <= cap_ctas)
   auto panels = [&](int64_t k, cudaStream_t s, int cap_ctas) -> int {
@@ -578,9 +616,9 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     stage_kernel<<<dim3(nL + nU + 2, np), 256, 0, s>>>(
         nL, nU, 1, (int)k, lslot, uslot, P->diag_slot[k], P->n_slots, P->n_pad, a->factor,
         a->pivots, stage_buf(k), pencil_stride);
-    const ItemMap pm{kMapPanel, nL, nU, nL + nU, 0, 0, nullptr, lslot, uslot};
+    const ItemMap pm{kMapPanel, nL, nU, nL + nU, 0, 0, nullptr, lslot, uslot, nullptr};
     schur_tc_kernel<<<grid_for((int64_t)(nL + nU) * np, cap_ctas), kPThreads, smem, s>>>(
-        pm, np, P->n_slots, stage_buf(k), pencil_stride, a->status, tmap_c);
+        pm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, tmap_c);
     count_launches(2);
     return 0;
   };
@@ -595,22 +633,114 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
                                                   pencil_stride);
     count_launches(1);
   };
-  // Schur update of step k (the pairs `kind` selects) on the caller stream
+  // Schur update of step k (the pairs `kind` selects) on stream s, untimed
+  auto schur_on = [&](int64_t k, int kind, int a0, int b0, int n_pairs, int cap_ctas,
+                      cudaStream_t s) {
+    const int nL = P->lb_off[k + 1] - P->lb_off[k];
+    const int nU = P->ur_off[k + 1] - P->ur_off[k];
+    const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr,
+                     nullptr};
+    schur_tc_kernel<<<grid_for((int64_t)n_pairs * np, cap_ctas), kPThreads, smem, s>>>(
+        sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, tmap_c);
+    count_launches(1);
+  };
+  // Schur update of step k (the pairs `kind` selects) on the caller stream,
+  // timed
   auto schur = [&](int64_t k, int kind, int a0, int b0, int n_pairs, int cap_ctas) {
     const int nL = P->lb_off[k + 1] - P->lb_off[k];
     const int nU = P->ur_off[k + 1] - P->ur_off[k];
     const int64_t items = (int64_t)n_pairs * np;
     cudaEvent_t ev[2];
     const bool timed = timing_begin(st, ev);
-    const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr};
+    const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr,
+                     nullptr};
     schur_tc_kernel<<<grid_for(items, cap_ctas), kPThreads, smem, st>>>(
-        sm, np, P->n_slots, stage_buf(k), pencil_stride, a->status, tmap_c);
+        sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, tmap_c);
     count_launches(1);
     if (timed)
       timing_end(kTimedSchur, st, ev, (double)items * 8.0 * kTcT * kTcT * kTcT,
                  (double)items * 2.0 * 2 * kTcT * kTcT * sizeof(float) +
                      (double)(nL + nU) * np * kStagedTileBytes * ((double)n_pairs / (nL * nU)));
   };
+
+  // targets of step k in tile row or column k + 1 (K = 128), on stream s
+  auto inner = [&](int64_t k, cudaStream_t s, int cap_ctas) {
+    const int nL = P->lb_off[k + 1] - P->lb_off[k];
+    const int nU = P->ur_off[k + 1] - P->ur_off[k];
+    if (nL == 0 || nU == 0) return;
+    const int a0 = P->lb_tile[P->lb_off[k]] == k + 1 ? 1 : 0;
+    const int b0 = P->ur_tile[P->ur_off[k]] == k + 1 ? 1 : 0;
+    const int cross = nL * nU - (nL - a0) * (nU - b0);
+    if (cross > 0) schur_on(k, kMapCross, a0, b0, cross, cap_ctas, s);
+  };
+  // two-step update of super-step ss (tile steps 2 ss, 2 ss + 1), the cross
+  // or the rest items, on the caller stream, timed
+  auto two_step = [&](int64_t ss, bool cross, int cap_ctas) {
+    const std::vector<int64_t>& off = cross ? P->ss_cross_off : P->ss_rest_off;
+    const std::vector<int32_t>& host = cross ? P->ss_cross : P->ss_rest;
+    const int32_t* dev = cross ? P->d_ss_cross : P->d_ss_rest;
+    const int64_t n = off[ss + 1] - off[ss];
+    if (n == 0) return;
+    const int64_t k0 = 2 * ss;
+    double halves = 0;
+    for (int64_t i = off[ss]; i < off[ss + 1]; ++i)
+      halves += (host[5 * i + 1] >= 0 ? 1 : 0) + (host[5 * i + 3] >= 0 ? 1 : 0);
+    cudaEvent_t ev[2];
+    const bool timed = timing_begin(st, ev);
+    const ItemMap lm{kMapList, 0, 0, (int)n, 0, 0, nullptr, nullptr, nullptr, dev + 5 * off[ss]};
+    schur_tc_kernel<<<grid_for(n * np, cap_ctas), kPThreads, smem, st>>>(
+        lm, np, P->n_slots, stage_buf(k0), stage_buf(k0 + 1), pencil_stride, a->status, tmap_c);
+    count_launches(1);
+    // algorithmic bytes: every target read and written once, the staged L
+    // and U tiles of both steps read once
+    const double staged = (double)(P->lb_off[k0 + 1] - P->lb_off[k0] + P->ur_off[k0 + 1] -
+                                   P->ur_off[k0] + P->lb_off[k0 + 2] - P->lb_off[k0 + 1] +
+                                   P->ur_off[k0 + 2] - P->ur_off[k0 + 1]);
+    if (timed)
+      timing_end(kTimedSchur, st, ev, halves * np * 8.0 * kTcT * kTcT * kTcT,
+                 (double)n * np * 2.0 * 2 * kTcT * kTcT * sizeof(float) +
+                     staged * np * kStagedTileBytes);
+  };
+
+  // Two-step (K = 256) updates with lookahead: per super-step (k, k + 1),
+  // after step k's cross targets (K = 128) and step k + 1's panels, one
+  // update applies both steps to every other target, reading and writing
+  // each target once instead of twice.  The items in tile rows/columns
+  // k + 2, k + 3 go first; the side stream then prepares the next
+  // super-step's two panels beside the rest.
+  const bool two_steps = tc_panels && lookahead && a->precision == AOSB_PRECISION_BF16X3 &&
+                         P->d_ss_rest != nullptr;
+  if (two_steps) {
+    const int64_t nb = P->nb;
+    if (int rc = panels(0, st, sms)) return rc;
+    stage_schur(0, st);
+    if (nb > 1) {
+      inner(0, st, sms);
+      if (int rc = panels(1, st, sms)) return rc;
+      stage_schur(1, st);
+    }
+    for (int64_t ss = 0; 2 * ss + 1 < nb; ++ss) {
+      const int64_t k2 = 2 * ss + 2, k3 = 2 * ss + 3;
+      two_step(ss, true, sms);
+      if (k2 < nb) {
+        AOSB_CUDA_TRY(cudaEventRecord(ev_cross, st), err, cap);
+        AOSB_CUDA_TRY(cudaStreamWaitEvent(side, ev_cross, 0), err, cap);
+        if (int rc = panels(k2, side, reserve)) return rc;
+        stage_schur(k2, side);
+        if (k3 < nb) {
+          inner(k2, side, reserve);
+          if (int rc = panels(k3, side, reserve)) return rc;
+          stage_schur(k3, side);
+        }
+        AOSB_CUDA_TRY(cudaEventRecord(ev_panel, side), err, cap);
+        two_step(ss, false, sms - reserve);
+        AOSB_CUDA_TRY(cudaStreamWaitEvent(st, ev_panel, 0), err, cap);
+      } else {
+        two_step(ss, false, sms);
+      }
+    }
+    return launch_check(err, cap, "tensor-core factorization");
+  }
 
   for (int64_t k = 0; k < P->nb; ++k) {
     const int nL = P->lb_off[k + 1] - P->lb_off[k];

@@ -15,6 +15,8 @@
 //    U tiles above and L tiles left, and the |L_k| x |U_k| Schur targets.
 #include "plan.h"
 
+#include <unordered_map>
+
 #include <algorithm>
 #include <deque>
 #include <numeric>
@@ -232,11 +234,74 @@ int plan_upload(aosb_plan* p, char* err, size_t cap) {
   return 0;
 }
 
+// Two-step Schur item lists (see plan.h).
+void build_super_steps(aosb_plan* P) {
+  const int64_t nb = P->nb;
+  P->ss_cross_off.assign(1, 0);
+  P->ss_rest_off.assign(1, 0);
+  P->ss_cross.clear();
+  P->ss_rest.clear();
+  struct Item {
+    int32_t i, j, slot, a0, b0, a1, b1;
+  };
+  std::vector<Item> items;
+  for (int64_t k0 = 0; k0 + 1 < nb; k0 += 2) {
+    const int64_t k1 = k0 + 1, k2 = k0 + 2, k3 = k0 + 3;
+    items.clear();
+    const int32_t l0 = P->lb_off[k0], nL0 = P->lb_off[k0 + 1] - l0;
+    const int32_t u0 = P->ur_off[k0], nU0 = P->ur_off[k0 + 1] - u0;
+    const int32_t l1 = P->lb_off[k1], nL1 = P->lb_off[k1 + 1] - l1;
+    const int32_t u1 = P->ur_off[k1], nU1 = P->ur_off[k1 + 1] - u1;
+    // dense index over the (i, j) targets of this super-step: i, j in
+    // [k2, nb) -> item position
+    std::unordered_map<int64_t, int32_t> at;
+    at.reserve((size_t)(nL0 * nU0 + nL1 * nU1) * 2 + 16);
+    auto get = [&](int32_t i, int32_t j) -> Item& {
+      const int64_t key = (int64_t)i * nb + j;
+      auto f = at.find(key);
+      if (f != at.end()) return items[f->second];
+      at.emplace(key, (int32_t)items.size());
+      items.push_back({i, j, P->slot[key], -1, -1, -1, -1});
+      return items.back();
+    };
+    for (int32_t a = 0; a < nL0; ++a) {
+      const int32_t i = P->lb_tile[l0 + a];
+      if (i == k1) continue;
+      for (int32_t b = 0; b < nU0; ++b) {
+        const int32_t j = P->ur_tile[u0 + b];
+        if (j == k1) continue;
+        Item& it = get(i, j);
+        it.a0 = a;
+        it.b0 = nL0 + b;
+      }
+    }
+    for (int32_t a = 0; a < nL1; ++a) {
+      const int32_t i = P->lb_tile[l1 + a];
+      for (int32_t b = 0; b < nU1; ++b) {
+        const int32_t j = P->ur_tile[u1 + b];
+        Item& it = get(i, j);
+        it.a1 = a;
+        it.b1 = nL1 + b;
+      }
+    }
+    std::sort(items.begin(), items.end(), [](const Item& x, const Item& y) {
+      return x.i != y.i ? x.i < y.i : x.j < y.j;
+    });
+    for (const Item& it : items) {
+      const bool cross = it.i == k2 || it.i == k3 || it.j == k2 || it.j == k3;
+      std::vector<int32_t>& dst = cross ? P->ss_cross : P->ss_rest;
+      dst.insert(dst.end(), {it.slot, it.a0, it.b0, it.a1, it.b1});
+    }
+    P->ss_cross_off.push_back((int64_t)P->ss_cross.size() / 5);
+    P->ss_rest_off.push_back((int64_t)P->ss_rest.size() / 5);
+  }
+}
+
 void plan_free_device(aosb_plan* p) {
   int32_t** arrs[] = {&p->d_perm, &p->d_pinv, &p->d_slot, &p->d_lb_slot, &p->d_ur_slot,
                       &p->d_ua_slot, &p->d_ll_slot, &p->d_lb_tile, &p->d_ur_tile,
                       &p->d_ua_tile, &p->d_ll_tile, &p->d_sc_slot, &p->d_diag_slot,
-                      &p->d_indices};
+                      &p->d_indices, &p->d_ss_cross, &p->d_ss_rest};
   for (int32_t** a : arrs) {
     if (*a) cudaFree(*a);
     *a = nullptr;
@@ -505,6 +570,7 @@ int aosb_plan_create(int64_t n, const int64_t* indptr, const int32_t* indices,
     }
     P->tree_levels = mx + 1;
   }
+  aosb::build_super_steps(P);
   P->h_indptr.assign(indptr, indptr + n + 1);
   P->h_indices.assign(indices, indices + nnz);
   *out = P;
@@ -516,6 +582,8 @@ int aosb_plan_upload(aosb_plan_t* P, char* err, size_t cap) {
   if (P->uploaded) return 0;
   int rc = aosb::plan_upload(P, err, cap);
   if (rc == 0) rc = aosb::up(&P->d_indptr, P->h_indptr, err, cap);
+  if (rc == 0 && !P->ss_cross.empty()) rc = aosb::up(&P->d_ss_cross, P->ss_cross, err, cap);
+  if (rc == 0 && !P->ss_rest.empty()) rc = aosb::up(&P->d_ss_rest, P->ss_rest, err, cap);
   if (rc == 0) rc = aosb::up(&P->d_indices, P->h_indices, err, cap);
   if (rc != 0) {
     aosb::plan_free_device(P);

@@ -21,11 +21,20 @@ struct aosb_plan {
   std::vector<int64_t> sc_off;                    // Schur target offsets [nb+1]
   std::vector<int32_t> sc_slot;                   // |L_k| x |U_k| target slots per step
   std::vector<int32_t> diag_slot;                 // slot of (k, k)
+  // Two-step (K = 256) Schur updates, super-step s = tile steps (2s, 2s+1):
+  // the targets of step 2s outside tile row/column 2s+1 merged with the
+  // targets of step 2s+1, 5 ints per item: target slot, then the staged A
+  // and B indices of step 2s (L index a, nL + U index b) or -1, then those of
+  // step 2s+1 or -1.  "cross" items lie in tile row or column 2s+2 or 2s+3
+  // (read by the next super-step's panels), "rest" items elsewhere.
+  std::vector<int64_t> ss_cross_off, ss_rest_off;  // [n_super + 1], in items
+  std::vector<int32_t> ss_cross, ss_rest;
   // Device copies.
   int32_t *d_perm = nullptr, *d_pinv = nullptr, *d_slot = nullptr;
   int32_t *d_lb_slot = nullptr, *d_ur_slot = nullptr, *d_ua_slot = nullptr, *d_ll_slot = nullptr;
   int32_t *d_lb_tile = nullptr, *d_ur_tile = nullptr, *d_ua_tile = nullptr, *d_ll_tile = nullptr;
   int32_t *d_sc_slot = nullptr, *d_diag_slot = nullptr;
+  int32_t *d_ss_cross = nullptr, *d_ss_rest = nullptr;
   // Pattern copies for the shifted-value assembly (host and device).
   std::vector<int64_t> h_indptr;
   std::vector<int32_t> h_indices;
@@ -38,4 +47,5 @@ namespace aosb {
 int plan_upload(aosb_plan* p, char* err, size_t cap);
 void plan_free_device(aosb_plan* p);
 void solve_graphs_forget(const aosb_plan* p);
+void build_super_steps(aosb_plan* p);
 }  // namespace aosb

@@ -431,8 +431,10 @@ class BandEngine:
     def precision_id(self) -> int:
         """The aosb_factor precision this engine's settings select."""
         if self.engine.precision == "mixed" and self.engine.tensor_cores:
-            return (native.PRECISION_BF16X3 if self.engine.tensor_core_panels
-                    else native.PRECISION_BF16X3_FP32_PANELS)
+            if not self.engine.tensor_core_panels:
+                return native.PRECISION_BF16X3_FP32_PANELS
+            return (native.PRECISION_BF16X3 if self.engine.schur_depth == 2
+                    else native.PRECISION_BF16X3_ONE_STEP)
         return native.PRECISION_PLAIN
 
     def _stream(self):

@@ -24,6 +24,7 @@ ERROR_CAPACITY = 512
 PRECISION_PLAIN = 0
 PRECISION_BF16X3 = 1
 PRECISION_BF16X3_FP32_PANELS = 2
+PRECISION_BF16X3_ONE_STEP = 3
 SOLVE_TENSOR_CORES = 1
 SOLVE_GRAPH = 2
 

@@ -63,6 +63,8 @@ def parse() -> argparse.Namespace:
                     default="auto", help="tile-plan ordering when not autotuned")
     ap.add_argument("--autotune", type=int, default=1,
                     help="1: time candidate tile plans and k-point batches on the device first")
+    ap.add_argument("--schur-depth", type=int, default=1, choices=(1, 2),
+                    help="tile steps per tensor-core Schur pass (2 = K 256)")
     ap.add_argument("--tensor-core-solves", type=int, default=-1,
                     help="1/0: split-BF16 tensor-core solve updates on/off (-1 = engine default)")
     return ap.parse_args()
@@ -325,6 +327,7 @@ def main() -> None:
                                     tensor_cores=bool(args.tensor_cores),
                                     autotune=bool(args.autotune),
                                     ordering=args.ordering,
+                                    schur_depth=args.schur_depth,
                                     max_pencils=args.max_pencils,
                                     **({"refinement_steps": args.refinement_steps}
                                        if args.refinement_steps >= 0 else {}),
@@ -464,6 +467,7 @@ def main() -> None:
                    "refinement_steps": eng.engine.refinement_steps if args.precision == "mixed"
                    else 0,
                    "tensor_core_solves": bool(eng.engine.tensor_core_solves),
+                   "schur_depth": eng.engine.schur_depth,
                    "autotune": tuning,
                    "factorizations_per_step": stats.get("factorizations"),
                    "pencil_batch": stats.get("pencil_batch"),

@@ -253,10 +253,13 @@ void aosb_plan_destroy(aosb_plan_t *plan);
  * diagonal.
  * ------------------------------------------------------------------------ */
 #define AOSB_PRECISION_PLAIN 0  /* complex64, FP32 SIMT updates */
-#define AOSB_PRECISION_BF16X3 1 /* split-BF16 tcgen05 panels and Schur updates,
+#define AOSB_PRECISION_BF16X3 1 /* split-BF16 tcgen05 panels and two-step
+                                   (K = 256) Schur updates with lookahead,
                                    FP32 accumulate (tile 128) */
 #define AOSB_PRECISION_BF16X3_FP32_PANELS 2 /* split-BF16 tcgen05 Schur updates,
                                                FP32 SIMT panels (tile 128) */
+#define AOSB_PRECISION_BF16X3_ONE_STEP 3 /* as 1 with one-step (K = 128) Schur
+                                            updates */
 
 typedef struct {
   uint32_t abi_version;

@@ -172,12 +172,13 @@ def test_plain_factor_solve_matches_superlu(case, tile, ordering, torch):
         plan.close()
 
 
-@pytest.mark.parametrize("precision,flags", [(1, 0), (2, 0), (1, 1)])
+@pytest.mark.parametrize("precision,flags", [(1, 0), (2, 0), (3, 0), (1, 1)])
 @pytest.mark.parametrize("case", ["small2d", "c1"])
 def test_tensor_core_factor_matches_superlu(case, precision, flags, torch):
-    """Split-BF16 tcgen05 Schur updates (precision 1: tensor-core panels
-    too; 2: FP32 SIMT panels; flags 1: tensor-core solve updates): unrefined
-    solves within 1e-3, FP64 refinement to 1e-9, both directions."""
+    """Split-BF16 tcgen05 Schur updates (precision 1: tensor-core panels and
+    two-step updates; 2: FP32 SIMT panels; 3: one-step updates; flags 1:
+    tensor-core solve updates): unrefined solves within 1e-3, FP64
+    refinement to 1e-9, both directions."""
     b = getattr(bundles, case)()
     dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[1], torch, 128)
     try:
@@ -398,6 +399,29 @@ def test_graph_replayed_solve_equals_direct(adjoint, torch):
             got = _factor_solve(dev, plan, h, s, shifts, rhs, torch, adjoint=adjoint, steps=1,
                                 flags=native.SOLVE_GRAPH)
             assert np.array_equal(got, ref)
+    finally:
+        dev.close()
+        plan.close()
+
+
+def test_two_step_factor_matches_one_step(torch):
+    """Two-step (K = 256) Schur updates give the factor of the one-step
+    updates up to split-BF16 rounding (same pivots on this pencil)."""
+    from aospectrum_b200 import native
+
+    b = bundles.c1()
+    dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[1], torch, 128, "natural")
+    try:
+        rng = np.random.default_rng(5)
+        rhs = (rng.standard_normal((dev.n, 4)) + 1j * rng.standard_normal((dev.n, 4)))
+        shifts = [-2.6 + 0.02j, -1.0 + 0.3j]
+        one = _factor_solve(dev, plan, h, s, shifts, rhs, torch,
+                            precision=native.PRECISION_BF16X3_ONE_STEP)
+        two = _factor_solve(dev, plan, h, s, shifts, rhs, torch,
+                            precision=native.PRECISION_BF16X3)
+        for p in range(len(shifts)):
+            rel = np.linalg.norm(two[p] - one[p]) / np.linalg.norm(one[p])
+            assert rel < 1e-3, (p, rel)
     finally:
         dev.close()
         plan.close()
