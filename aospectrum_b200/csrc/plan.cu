@@ -624,6 +624,20 @@ int aosb_plan_export_slots(const aosb_plan_t* p, int32_t* slot) {
   return 0;
 }
 
+int aosb_plan_export_super_steps(const aosb_plan_t* p, int64_t* n_super, int64_t* n_cross,
+                                 int64_t* n_rest, int64_t* cross_off, int64_t* rest_off,
+                                 int32_t* cross, int32_t* rest) {
+  if (p == nullptr) return AOSB_ERR_NULL;
+  if (n_super) *n_super = (int64_t)p->ss_cross_off.size() - 1;
+  if (n_cross) *n_cross = (int64_t)p->ss_cross.size() / 5;
+  if (n_rest) *n_rest = (int64_t)p->ss_rest.size() / 5;
+  if (cross_off) std::copy(p->ss_cross_off.begin(), p->ss_cross_off.end(), cross_off);
+  if (rest_off) std::copy(p->ss_rest_off.begin(), p->ss_rest_off.end(), rest_off);
+  if (cross) std::copy(p->ss_cross.begin(), p->ss_cross.end(), cross);
+  if (rest) std::copy(p->ss_rest.begin(), p->ss_rest.end(), rest);
+  return 0;
+}
+
 void aosb_plan_destroy(aosb_plan_t* p) {
   if (p == nullptr) return;
   aosb::solve_graphs_forget(p);

@@ -119,6 +119,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_plan_info": (C.c_int, [c_vp, C.POINTER(PlanInfo)]),
     "aosb_plan_export_perm": (C.c_int, [c_vp, c_vp]),
     "aosb_plan_export_slots": (C.c_int, [c_vp, c_vp]),
+    "aosb_plan_export_super_steps": (C.c_int, [c_vp, C.POINTER(c_i64), C.POINTER(c_i64),
+                                               C.POINTER(c_i64), c_vp, c_vp, c_vp, c_vp]),
     "aosb_plan_destroy": (None, [c_vp]),
     "aosb_factor_bytes": (c_sz, [c_vp, c_i32]),
     "aosb_factor_workspace_bytes": (c_sz, [c_vp, c_i32, c_i32]),

@@ -243,6 +243,14 @@ int aosb_plan_info(const aosb_plan_t *plan, aosb_plan_info_v1 *info);
 int aosb_plan_export_perm(const aosb_plan_t *plan, int32_t *perm);
 /* slot[n_tiles*n_tiles]: storage slot of each tile, -1 if structurally 0. */
 int aosb_plan_export_slots(const aosb_plan_t *plan, int32_t *slot);
+/* The two-step (K = 256) Schur item lists of the plan (host copies), for
+ * inspection and tests; no counterpart in the reference.  Call with null
+ * arrays for the sizes: n_super super-steps (tile steps 2s, 2s+1),
+ * cross_off / rest_off [n_super + 1] item offsets, items of 5 ints (target
+ * slot, staged A and B index of step 2s or -1, of step 2s+1 or -1). */
+int aosb_plan_export_super_steps(const aosb_plan_t *plan, int64_t *n_super, int64_t *n_cross,
+                                 int64_t *n_rest, int64_t *cross_off, int64_t *rest_off,
+                                 int32_t *cross, int32_t *rest);
 void aosb_plan_destroy(aosb_plan_t *plan);
 
 /* ------------------------------------------------------------------------

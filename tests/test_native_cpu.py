@@ -130,6 +130,66 @@ def test_symbolic_plan_is_a_closed_fill_pattern(name, tile, ordering):
     lib.aosb_plan_destroy(h)
 
 
+@pytest.mark.parametrize("name,tile,ordering", [("c1", 32, 1), ("c1", 64, 0), ("small2d", 32, 0)])
+def test_two_step_schur_lists_cover_both_steps(name, tile, ordering):
+    """Super-step s = tile steps (k0, k1) = (2s, 2s + 1): the K = 256 items
+    hold exactly step k0's Schur targets outside tile row/column k1 (those go
+    to the K = 128 "inner" update) and all of step k1's targets, with the
+    staged operand indices of the step lists; "cross" items are exactly the
+    ones in tile rows/columns k0 + 2, k0 + 3."""
+    b = getattr(bundles, name)()
+    pat = bloch_ref.build_pattern(b)
+    rc, h, msg = _plan(pat.indptr, pat.indices, b.n_orbitals, tile, ordering,
+                       np.ascontiguousarray(b.basis.atom_offsets, np.int64))
+    assert rc == 0, msg
+    lib = native.library()
+    info = native.PlanInfo()
+    lib.aosb_plan_info(h, C.byref(info))
+    nb = info.n_tiles
+    slot = np.empty(nb * nb, np.int32)
+    lib.aosb_plan_export_slots(h, slot.ctypes.data)
+    slot = slot.reshape(nb, nb)
+    ns, nc, nr = C.c_int64(), C.c_int64(), C.c_int64()
+    lib.aosb_plan_export_super_steps(h, C.byref(ns), C.byref(nc), C.byref(nr), None, None, None,
+                                     None)
+    assert ns.value == nb // 2
+    coff = np.empty(ns.value + 1, np.int64)
+    roff = np.empty(ns.value + 1, np.int64)
+    cross = np.empty(5 * max(nc.value, 1), np.int32)
+    rest = np.empty(5 * max(nr.value, 1), np.int32)
+    lib.aosb_plan_export_super_steps(h, None, None, None, coff.ctypes.data, roff.ctypes.data,
+                                     cross.ctypes.data, rest.ctypes.data)
+    cross, rest = cross[:5 * nc.value].reshape(-1, 5), rest[:5 * nr.value].reshape(-1, 5)
+    where = {int(slot[i, j]): (i, j) for i in range(nb) for j in range(nb) if slot[i, j] >= 0}
+    nonempty = 0
+    for s in range(ns.value):
+        k0, k1 = 2 * s, 2 * s + 1
+        L0 = [i for i in range(k0 + 1, nb) if slot[i, k0] >= 0]
+        U0 = [j for j in range(k0 + 1, nb) if slot[k0, j] >= 0]
+        L1 = [i for i in range(k1 + 1, nb) if slot[i, k1] >= 0]
+        U1 = [j for j in range(k1 + 1, nb) if slot[k1, j] >= 0]
+        want = {}
+        for a, i in enumerate(L0):
+            for bb, j in enumerate(U0):
+                if i != k1 and j != k1:
+                    want.setdefault((i, j), [-1, -1, -1, -1])[0:2] = [a, len(L0) + bb]
+        for a, i in enumerate(L1):
+            for bb, j in enumerate(U1):
+                want.setdefault((i, j), [-1, -1, -1, -1])[2:4] = [a, len(L1) + bb]
+        got = {}
+        for part, items in (("cross", cross[coff[s]:coff[s + 1]]), ("rest", rest[roff[s]:roff[s + 1]])):
+            for it in items:
+                i, j = where[int(it[0])]
+                assert (i, j) not in got
+                in_cross = i in (k0 + 2, k0 + 3) or j in (k0 + 2, k0 + 3)
+                assert in_cross == (part == "cross"), (s, i, j, part)
+                got[(i, j)] = [int(v) for v in it[1:]]
+        assert got == want, s
+        nonempty += len(got) > 0
+    assert nonempty > 0
+    lib.aosb_plan_destroy(h)
+
+
 def test_symbolic_plan_rejects_bad_patterns():
     ip = np.array([0, 2, 3], np.int64)
     assert _plan(ip, np.array([0, 1, 0], np.int32), 2)[0] == 33      # row 1 misses its diagonal
