@@ -114,7 +114,7 @@ class EngineSettings:
     tensor_core_panels: bool = True
     tensor_core_solves: bool = True
     autotune: bool = False
-    schur_depth: int = 1
+    schur_depth: int = 2
     cuda_graphs: bool = False
 
     def __post_init__(self) -> None:

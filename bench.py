@@ -63,7 +63,7 @@ def parse() -> argparse.Namespace:
                     default="auto", help="tile-plan ordering when not autotuned")
     ap.add_argument("--autotune", type=int, default=1,
                     help="1: time candidate tile plans and k-point batches on the device first")
-    ap.add_argument("--schur-depth", type=int, default=1, choices=(1, 2),
+    ap.add_argument("--schur-depth", type=int, default=2, choices=(1, 2),
                     help="tile steps per tensor-core Schur pass (2 = K 256)")
     ap.add_argument("--tensor-core-solves", type=int, default=-1,
                     help="1/0: split-BF16 tensor-core solve updates on/off (-1 = engine default)")
