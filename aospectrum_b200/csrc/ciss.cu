@@ -6,8 +6,10 @@
 // norms.  Here they run on the device in FP64 so that the projected
 // problems and the reported residuals carry FP64 accuracy.
 #include "common.cuh"
+#include "timing.h"
 
 #include <mutex>
+#include <vector>
 
 namespace aosb {
 namespace {
@@ -210,9 +212,29 @@ int aosb_spmm(int64_t n, int32_t ncols, const int64_t* indptr, const int32_t* in
     return aosb::set_error(err, cap, AOSB_ERR_NULL, "null argument");
   if (n <= 0 || ncols <= 0 || ldx < ncols || ldy < ncols)
     return aosb::set_error(err, cap, AOSB_ERR_ARGUMENT, "invalid spmm shape");
+  cudaEvent_t ev[2];
+  const bool timed = aosb::timing_begin((cudaStream_t)stream, ev);
   aosb::spmm_kernel<<<aosb::ceil_div(n, 8), 256, 0, (cudaStream_t)stream>>>(
       n, ncols, indptr, indices, (const float2*)values, (const double2*)x, ldx, (double2*)y, ldy);
   aosb::count_launches(1);
+  if (timed) {
+    // nnz of a pattern, read once per indptr array (timing runs only)
+    static std::mutex mu;
+    static std::vector<std::pair<const int64_t*, int64_t>> seen;
+    int64_t nnz = -1;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      for (auto& e : seen)
+        if (e.first == indptr + n) nnz = e.second;
+    }
+    if (nnz < 0) {
+      cudaMemcpy(&nnz, indptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost);
+      std::lock_guard<std::mutex> lock(mu);
+      seen.emplace_back(indptr + n, nnz);
+    }
+    aosb::timing_end(aosb::kTimedSpmm, (cudaStream_t)stream, ev, 8.0 * nnz * ncols,
+                     12.0 * nnz + (double)n * ncols * 32.0);
+  }
   return aosb::launch_check(err, cap, "spmm");
 }
 

@@ -655,11 +655,18 @@ int aosb_shifted_residual_blocks(int64_t n, int32_t nrhs, int32_t np, int64_t n_
   const int ncs = (nrhs + 31) / 32;
   if (n_blocks * ncs > INT32_MAX) return aosb::set_error(err, cap, AOSB_ERR_SIZE, "too many row blocks");
   dim3 g((unsigned)(n_blocks * ncs), np);
+  cudaEvent_t ev[2];
+  const bool timed = aosb::timing_begin((cudaStream_t)stream, ev);
   aosb::shifted_residual_blocks_kernel<<<g, aosb::kResWarps * 32, 0, (cudaStream_t)stream>>>(
       n_blocks, row_blocks, nrhs, indptr, indices, (const float2*)h_values,
       (const float2*)s_values, nnz, pencil_k, (const double2*)shifts, (const double2*)b,
       b_stride, (const double2*)x, (double2*)r, n);
   aosb::count_launches(1);
+  // algorithmic: 8 FP64 flops per (nonzero, column, pencil); H and S values
+  // once per k, x read and r written once per pencil
+  if (timed)
+    aosb::timing_end(aosb::kTimedResidual, (cudaStream_t)stream, ev, 8.0 * nnz * nrhs * np,
+                     16.0 * nnz + (double)np * n * nrhs * 16.0 * 3.0);
   return aosb::launch_check(err, cap, "shifted_residual_blocks");
 }
 

@@ -11,7 +11,9 @@ enum TimedKernel : int {
   kTimedSchur = 0,        // schur_tc_kernel, Schur items
   kTimedSolveDiag = 1,    // solve_diag_kernel
   kTimedSolveUpdate = 2,  // solve_update_kernel / solve_tc_kernel
-  kTimedCount = 3,
+  kTimedResidual = 3,     // shifted_residual(_blocks)_kernel
+  kTimedSpmm = 4,         // spmm_kernel
+  kTimedCount = 5,
 };
 
 // Records a start event on `st` and returns true when timing is on (and the

@@ -391,7 +391,8 @@ def main() -> None:
     native.library().aosb_kernel_timing_read(native.C.byref(k_ms), native.C.byref(k_flops),
                                              native.C.byref(k_bytes), native.C.byref(k_launches))
     breakdown = {}
-    for cat, name in ((1, "solve_diag"), (2, "solve_update")):
+    for cat, name in ((1, "solve_diag"), (2, "solve_update"), (3, "fp64_residual"),
+                      (4, "fp64_spmm")):
         c_ms, c_fl, c_by, c_n = (native.C.c_double(), native.C.c_double(), native.C.c_double(),
                                  native.c_i64())
         native.library().aosb_kernel_timing_read_category(

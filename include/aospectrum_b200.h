@@ -92,7 +92,9 @@ int aosb_kernel_timing_read(double *total_ms, double *flops, double *bytes,
 /* The same for a category: 0 = tensor-core Schur updates, 1 = solve
  * diagonal steps (4 T^2 L flops per pencil), 2 = solve tile updates
  * (8 T^2 L flops per tile and pencil; factor tile read, X tile read and
- * written).  Timing skips launches issued while a stream is captured. */
+ * written), 3 = FP64 shifted residuals (8 flops per nonzero, column and
+ * pencil), 4 = FP64 SpMM (8 flops per nonzero and column).  Timing skips
+ * launches issued while a stream is captured. */
 int aosb_kernel_timing_read_category(int32_t category, double *total_ms, double *flops,
                                      double *bytes, int64_t *launches);
 
