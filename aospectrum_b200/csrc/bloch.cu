@@ -15,6 +15,7 @@
 // real block values the products v * phase are exact, so the output is
 // bit-identical to the reference's numpy path.
 #include "common.cuh"
+#include "timing.h"
 
 #include <algorithm>
 #include <numeric>
@@ -43,6 +44,7 @@ struct aosb_bloch {
   std::vector<int32_t> pairs;
   std::vector<int64_t> m_off;
   std::vector<int32_t> m_shift;
+  int64_t n_values = 0;  // stored block values (sum of block sizes), set at upload
   bool uploaded = false;
 };
 
@@ -311,6 +313,10 @@ int aosb_bloch_upload(aosb_bloch_t* B, char* err, size_t cap) {
       (rc = upload(&B->d_member_off, B->m_off, err, cap)) ||
       (rc = upload(&B->d_member_shift, B->m_shift, err, cap)))
     return rc;
+  int64_t values = 0;
+  for (size_t g = 0; g < B->g_info.size(); ++g)
+    values += (int64_t)B->g_info[g].x * B->g_info[g].y * (B->g_mem[g].y - B->g_mem[g].x);
+  B->n_values = values;
   B->uploaded = true;
   return 0;
 }
@@ -356,6 +362,8 @@ int aosb_bloch_apply(const aosb_bloch_t* b, int32_t value_kind, const void* h_va
   dim3 grid(aosb::ceil_div(b->n_pairs, warps), n_k);
   cudaStream_t st = (cudaStream_t)stream;
   const int64_t nsh = (int64_t)(b->shifts.size() / 3);
+  cudaEvent_t ev[2];
+  const bool timed = aosb::timing_begin(st, ev);
   if (value_kind == 0) {
     bloch_pairs_kernel<float><<<grid, warps * 32, 0, st>>>(
         b->n_pairs, b->d_pairs, b->d_group, b->d_group_dst, b->d_group_members, b->d_member_off,
@@ -370,6 +378,12 @@ int aosb_bloch_apply(const aosb_bloch_t* b, int32_t value_kind, const void* h_va
     return aosb::set_error(err, cap, AOSB_ERR_ARGUMENT, "value_kind must be 0 or 1");
   }
   aosb::count_launches(1);
+  // algorithmic bytes per k: the stored H and S block values read once, the
+  // complex64 H(k) and S(k) CSR values written once
+  if (timed)
+    aosb::timing_end(aosb::kTimedBloch, st, ev, 0.0,
+                     (double)n_k * ((double)b->n_values * 2.0 * (value_kind ? 8.0 : 4.0) +
+                                    (double)b->nnz * 2.0 * 8.0));
   return aosb::launch_check(err, cap, "bloch_pairs_kernel");
 }
 

@@ -13,7 +13,8 @@ enum TimedKernel : int {
   kTimedSolveUpdate = 2,  // solve_update_kernel / solve_tc_kernel
   kTimedResidual = 3,     // shifted_residual(_blocks)_kernel
   kTimedSpmm = 4,         // spmm_kernel
-  kTimedCount = 5,
+  kTimedBloch = 5,        // bloch_pairs_kernel
+  kTimedCount = 6,
 };
 
 // Records a start event on `st` and returns true when timing is on (and the

@@ -391,8 +391,10 @@ def main() -> None:
     native.library().aosb_kernel_timing_read(native.C.byref(k_ms), native.C.byref(k_flops),
                                              native.C.byref(k_bytes), native.C.byref(k_launches))
     breakdown = {}
+    peaks_hbm = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0) \
+        if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
     for cat, name in ((1, "solve_diag"), (2, "solve_update"), (3, "fp64_residual"),
-                      (4, "fp64_spmm")):
+                      (4, "fp64_spmm"), (5, "bloch_sum")):
         c_ms, c_fl, c_by, c_n = (native.C.c_double(), native.C.c_double(), native.C.c_double(),
                                  native.c_i64())
         native.library().aosb_kernel_timing_read_category(
@@ -402,6 +404,8 @@ def main() -> None:
             breakdown[name] = {"ms_per_step": c_ms.value / args.steps, "launches": int(c_n.value),
                                "avg_launch_us": 1e3 * c_ms.value / c_n.value,
                                "gbs": c_by.value / (c_ms.value / 1e3) / 1e9,
+                               "hbm_frac": (c_by.value / (c_ms.value / 1e3) / 1e9) /
+                               peaks_hbm,
                                "tflops": c_fl.value / (c_ms.value / 1e3) / 1e12}
     breakdown["schur_tc"] = {"ms_per_step": k_ms.value / args.steps,
                              "launches": int(k_launches.value)}

@@ -93,8 +93,10 @@ int aosb_kernel_timing_read(double *total_ms, double *flops, double *bytes,
  * diagonal steps (4 T^2 L flops per pencil), 2 = solve tile updates
  * (8 T^2 L flops per tile and pencil; factor tile read, X tile read and
  * written), 3 = FP64 shifted residuals (8 flops per nonzero, column and
- * pencil), 4 = FP64 SpMM (8 flops per nonzero and column).  Timing skips
- * launches issued while a stream is captured. */
+ * pencil), 4 = FP64 SpMM (8 flops per nonzero and column), 5 = Bloch sums
+ * (bytes: stored H and S values read once, complex64 H(k), S(k) written
+ * once per k point).  Timing skips launches issued while a stream is
+ * captured. */
 int aosb_kernel_timing_read_category(int32_t category, double *total_ms, double *flops,
                                      double *bytes, int64_t *launches);
 
