@@ -8,10 +8,11 @@
 // CSR arrays, because every row of atom i has the same column structure.
 // Entry (a, c) of group (i, j) sits at dst_base + a * rowlen_i + c.
 //
-// The device kernel gives one warp to each unordered atom pair {i, j}: it
-// sums the member blocks of (i, j) and of its mirror (j, i) in block order
-// (the order the reference's stable sort leaves them in), applies the
-// Hermitian projection of sparse.py:25-36 and writes both windows.  With
+// The device kernel gives one warp to each unordered atom pair {i, j} and
+// chunk of up to four k points: it sums the member blocks of (i, j) and of
+// its mirror (j, i) in block order (the order the reference's stable sort
+// leaves them in), applies the Hermitian projection of sparse.py:25-36 and
+// writes both windows row by row for every k point of the chunk.  With
 // real block values the products v * phase are exact, so the output is
 // bit-identical to the reference's numpy path.
 #include "common.cuh"
@@ -84,75 +85,125 @@ __device__ __forceinline__ float2 cmul_rn(float2 a, float2 b) {
                      __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
 }
 
+// k points per warp: one warp reads its blocks once and writes this many
+// H(k), S(k) windows (four keeps the kernel at 64 registers, 32 warps per SM)
+constexpr int kBlochKChunk = 4;
+
+// Sums of one element over the member blocks [range.x, range.y) of a group
+// for the k points k0 .. k0+nk-1 (nk <= kBlochKChunk): each member value is
+// loaded once and multiplied by the phase of its lattice shift at every k.
+// Members are added in block order, first product first, for every k.
 template <typename V>
-__device__ __forceinline__ float2 group_sum(const V* vals, const int64_t* moff, const int32_t* msh,
-                                            const float2* ph, int2 range, int64_t elem) {
-  float2 s = make_float2(0.0f, 0.0f);
+__device__ __forceinline__ void group_sums(const V* vals, const int64_t* moff, const int32_t* msh,
+                                           const float2* ph0, int64_t n_shifts, int nk,
+                                           int2 range, int64_t elem,
+                                           float2 (&s)[kBlochKChunk]) {
+#pragma unroll
+  for (int q = 0; q < kBlochKChunk; ++q) s[q] = make_float2(0.0f, 0.0f);
   for (int m = range.x; m < range.y; ++m) {
-    float2 p = cmul_rn(load_value<V>(vals, moff[m] + elem), ph[msh[m]]);
-    if (m == range.x) {
-      s = p;
-    } else {
-      s.x = __fadd_rn(s.x, p.x);
-      s.y = __fadd_rn(s.y, p.y);
+    const float2 v = load_value<V>(vals, moff[m] + elem);
+    const float2* ph = ph0 + msh[m];
+#pragma unroll
+    for (int q = 0; q < kBlochKChunk; ++q) {
+      if (q < nk) {
+        const float2 p = cmul_rn(v, ph[q * n_shifts]);
+        if (m == range.x) {
+          s[q] = p;
+        } else {
+          s[q].x = __fadd_rn(s[q].x, p.x);
+          s[q].y = __fadd_rn(s[q].y, p.y);
+        }
+      }
     }
   }
-  return s;
 }
 
+__device__ __forceinline__ float2 hermitian_mean(float2 x, float2 y) {
+  return make_float2(__fmul_rn(__fadd_rn(x.x, y.x), 0.5f), __fmul_rn(__fsub_rn(x.y, y.y), 0.5f));
+}
+
+// Output element (a, c) of window (i, j) and the conjugate entry (c, a) of
+// window (j, i) need the same Hermitian mean; the kernel recomputes the mean
+// for each window so that every lane writes along window rows (coalesced)
+// instead of transposed.
 template <typename V>
-__global__ void __launch_bounds__(256) bloch_pairs_kernel(
+__global__ void __launch_bounds__(256, 4) bloch_pairs_kernel(
     int64_t n_pairs, const int32_t* __restrict__ pairs, const int4* __restrict__ group,
     const int64_t* __restrict__ gdst, const int2* __restrict__ gmem,
     const int64_t* __restrict__ moff, const int32_t* __restrict__ msh,
     const V* __restrict__ hv, const V* __restrict__ sv, const float2* __restrict__ phases,
-    int64_t n_shifts, int64_t nnz, float2* __restrict__ hout, float2* __restrict__ sout) {
+    int64_t n_shifts, int64_t nnz, int n_k, float2* __restrict__ hout,
+    float2* __restrict__ sout) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (warp >= n_pairs) return;
-  const int kk = blockIdx.y;
-  const float2* ph = phases + (int64_t)kk * n_shifts;
-  float2* ho = hout + (int64_t)kk * nnz;
-  float2* so = sout + (int64_t)kk * nnz;
+  const int k0 = blockIdx.y * kBlochKChunk;
+  const int nk = min(n_k - k0, kBlochKChunk);
+  const float2* ph0 = phases + (int64_t)k0 * n_shifts;
+  const int64_t out0 = (int64_t)k0 * nnz;
   const int g = pairs[warp];
   const int4 gi = group[g];  // nr, nc, rowlen, mirror
   const int nr = gi.x, nc = gi.y, rl = gi.z, gm = gi.w;
+  const int ne = nr * nc;
   const int64_t base = gdst[g];
   const int2 rg = gmem[g];
+  float2 x[kBlochKChunk], y[kBlochKChunk];
   if (gm != g) {
     const int4 mi = group[gm];
     const int64_t mbase = gdst[gm];
     const int2 mr = gmem[gm];
-    for (int e = lane; e < nr * nc; e += 32) {
-      const int a = e / nc, c = e - (e / nc) * nc;
-      const int64_t melem = (int64_t)c * nr + a;
-      for (int which = 0; which < 2; ++which) {
-        const V* vals = which == 0 ? hv : sv;
-        float2* out = which == 0 ? ho : so;
-        float2 x = group_sum<V>(vals, moff, msh, ph, rg, e);
-        float2 y = group_sum<V>(vals, moff, msh, ph, mr, melem);
-        float2 mean = make_float2(__fmul_rn(__fadd_rn(x.x, y.x), 0.5f),
-                                  __fmul_rn(__fsub_rn(x.y, y.y), 0.5f));
-        out[base + (int64_t)a * rl + c] = mean;
-        out[mbase + (int64_t)c * mi.z + a] = make_float2(mean.x, -mean.y);
+    // t runs over [matrix H|S][window (i,j)|(j,i)][row-major element]
+    for (int t = lane; t < 4 * ne; t += 32) {
+      const int which = t >= 2 * ne;
+      const int r = t - which * 2 * ne;
+      const int win = r >= ne;
+      const int e = r - win * ne;
+      int a, c;
+      int64_t dst;
+      if (win == 0) {
+        a = e / nc;
+        c = e - a * nc;
+        dst = base + (int64_t)a * rl + c;
+      } else {
+        c = e / nr;
+        a = e - c * nr;
+        dst = mbase + (int64_t)c * mi.z + a;
+      }
+      const V* vals = which == 0 ? hv : sv;
+      float2* out = (which == 0 ? hout : sout) + out0 + dst;
+      group_sums<V>(vals, moff, msh, ph0, n_shifts, nk, rg, a * nc + c, x);
+      group_sums<V>(vals, moff, msh, ph0, n_shifts, nk, mr, c * nr + a, y);
+#pragma unroll
+      for (int q = 0; q < kBlochKChunk; ++q) {
+        if (q < nk) {
+          const float2 mean = hermitian_mean(x[q], y[q]);
+          out[q * nnz] = win == 0 ? mean : make_float2(mean.x, -mean.y);
+        }
       }
     }
   } else {
-    for (int e = lane; e < nr * nc; e += 32) {
+    // t runs over [matrix H|S][row-major element]; the mean of the pair
+    // (lo, hi) is formed the same way for both of its entries
+    for (int t = lane; t < 2 * ne; t += 32) {
+      const int which = t >= ne;
+      const int e = t - which * ne;
       const int a = e / nc, c = e - (e / nc) * nc;
-      if (a > c) continue;
-      for (int which = 0; which < 2; ++which) {
-        const V* vals = which == 0 ? hv : sv;
-        float2* out = which == 0 ? ho : so;
-        float2 x = group_sum<V>(vals, moff, msh, ph, rg, e);
-        if (a == c) {
-          out[base + (int64_t)a * rl + c] = make_float2(x.x, 0.0f);
-        } else {
-          float2 y = group_sum<V>(vals, moff, msh, ph, rg, (int64_t)c * nc + a);
-          float2 mean = make_float2(__fmul_rn(__fadd_rn(x.x, y.x), 0.5f),
-                                    __fmul_rn(__fsub_rn(x.y, y.y), 0.5f));
-          out[base + (int64_t)a * rl + c] = mean;
-          out[base + (int64_t)c * rl + a] = make_float2(mean.x, -mean.y);
+      const V* vals = which == 0 ? hv : sv;
+      float2* out = (which == 0 ? hout : sout) + out0 + base + (int64_t)a * rl + c;
+      const int lo = min(a, c), hi = max(a, c);
+      group_sums<V>(vals, moff, msh, ph0, n_shifts, nk, rg, lo * nc + hi, x);
+      if (a != c) group_sums<V>(vals, moff, msh, ph0, n_shifts, nk, rg, hi * nc + lo, y);
+#pragma unroll
+      for (int q = 0; q < kBlochKChunk; ++q) {
+        if (q < nk) {
+          float2 v;
+          if (a == c) {
+            v = make_float2(x[q].x, 0.0f);
+          } else {
+            const float2 mean = hermitian_mean(x[q], y[q]);
+            v = a < c ? mean : make_float2(mean.x, -mean.y);
+          }
+          out[q * nnz] = v;
         }
       }
     }
@@ -359,7 +410,7 @@ int aosb_bloch_apply(const aosb_bloch_t* b, int32_t value_kind, const void* h_va
   if (n_k <= 0 || n_k > 65535)
     return aosb::set_error(err, cap, AOSB_ERR_ARGUMENT, "n_k must be in 1..65535");
   const int warps = 8;
-  dim3 grid(aosb::ceil_div(b->n_pairs, warps), n_k);
+  dim3 grid(aosb::ceil_div(b->n_pairs, warps), aosb::ceil_div(n_k, kBlochKChunk));
   cudaStream_t st = (cudaStream_t)stream;
   const int64_t nsh = (int64_t)(b->shifts.size() / 3);
   cudaEvent_t ev[2];
@@ -368,22 +419,22 @@ int aosb_bloch_apply(const aosb_bloch_t* b, int32_t value_kind, const void* h_va
     bloch_pairs_kernel<float><<<grid, warps * 32, 0, st>>>(
         b->n_pairs, b->d_pairs, b->d_group, b->d_group_dst, b->d_group_members, b->d_member_off,
         b->d_member_shift, (const float*)h_values, (const float*)s_values,
-        (const float2*)phases, nsh, b->nnz, (float2*)h_out, (float2*)s_out);
+        (const float2*)phases, nsh, b->nnz, n_k, (float2*)h_out, (float2*)s_out);
   } else if (value_kind == 1) {
     bloch_pairs_kernel<float2><<<grid, warps * 32, 0, st>>>(
         b->n_pairs, b->d_pairs, b->d_group, b->d_group_dst, b->d_group_members, b->d_member_off,
         b->d_member_shift, (const float2*)h_values, (const float2*)s_values,
-        (const float2*)phases, nsh, b->nnz, (float2*)h_out, (float2*)s_out);
+        (const float2*)phases, nsh, b->nnz, n_k, (float2*)h_out, (float2*)s_out);
   } else {
     return aosb::set_error(err, cap, AOSB_ERR_ARGUMENT, "value_kind must be 0 or 1");
   }
   aosb::count_launches(1);
-  // algorithmic bytes per k: the stored H and S block values read once, the
-  // complex64 H(k) and S(k) CSR values written once
+  // algorithmic bytes: the stored H and S block values read once per launch,
+  // the complex64 H(k) and S(k) CSR values written once per k point
   if (timed)
     aosb::timing_end(aosb::kTimedBloch, st, ev, 0.0,
-                     (double)n_k * ((double)b->n_values * 2.0 * (value_kind ? 8.0 : 4.0) +
-                                    (double)b->nnz * 2.0 * 8.0));
+                     (double)b->n_values * 2.0 * (value_kind ? 8.0 : 4.0) +
+                         (double)n_k * (double)b->nnz * 2.0 * 8.0);
   return aosb::launch_check(err, cap, "bloch_pairs_kernel");
 }
 

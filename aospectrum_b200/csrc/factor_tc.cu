@@ -78,24 +78,34 @@ __host__ __device__ __forceinline__ uint32_t staged_offset(int row, int k, int p
 //              zeros below (inv(U_kk))
 enum StageKind : int { kStageA = 0, kStageB = 1, kStageBPerm = 2, kStageAUnitLower = 3, kStageBUpper = 4 };
 
+__device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
 __device__ __forceinline__ void stage_tile(const float* __restrict__ F, unsigned char* __restrict__ out,
                                            int kind, const int32_t* __restrict__ pv) {
   const bool a_side = kind == kStageA || kind == kStageAUnitLower;
-  // Each thread converts pairs of consecutive k for one operand row, so a
-  // 4-byte store writes two BF16 values.
-  for (int e = threadIdx.x; e < kTcT * (kTcT / 2); e += blockDim.x) {
-    int row, k;
-    float re[2], im[2];
+  // Each thread converts 8 consecutive k of one operand row into one 16-byte
+  // chunk of every plane.  Consecutive threads take consecutive operand rows,
+  // whose chunks are adjacent in the staged layout, so a warp stores 512
+  // contiguous bytes per plane; A-side reads are whole 32-byte row segments,
+  // B-side reads are 128-byte row runs of the tile.
+  for (int e = threadIdx.x; e < kTcT * (kTcT / 8); e += blockDim.x) {
+    const int row = e % kTcT;
+    const int k0 = (e / kTcT) * 8;
+    float re[8], im[8];
     if (a_side) {
-      row = e / (kTcT / 2);
-      k = (e % (kTcT / 2)) * 2;
-      const size_t o = (size_t)row * kTcT + k;
-      re[0] = F[o]; re[1] = F[o + 1];
-      im[0] = F[o + kTcT * kTcT]; im[1] = F[o + 1 + kTcT * kTcT];
+      const float4* sr = reinterpret_cast<const float4*>(F + (size_t)row * kTcT + k0);
+      const float4* si = reinterpret_cast<const float4*>(F + kTcT * kTcT + (size_t)row * kTcT + k0);
+      const float4 r0 = sr[0], r1 = sr[1], i0 = si[0], i1 = si[1];
+      re[0] = r0.x; re[1] = r0.y; re[2] = r0.z; re[3] = r0.w;
+      re[4] = r1.x; re[5] = r1.y; re[6] = r1.z; re[7] = r1.w;
+      im[0] = i0.x; im[1] = i0.y; im[2] = i0.z; im[3] = i0.w;
+      im[4] = i1.x; im[5] = i1.y; im[6] = i1.z; im[7] = i1.w;
       if (kind == kStageAUnitLower) {
 #pragma unroll
-        for (int t = 0; t < 2; ++t) {
-          const int q = k + t;
+        for (int t = 0; t < 8; ++t) {
+          const int q = k0 + t;
           if (q >= row) {
             re[t] = q == row ? 1.0f : 0.0f;
             im[t] = 0.0f;
@@ -103,35 +113,39 @@ __device__ __forceinline__ void stage_tile(const float* __restrict__ F, unsigned
         }
       }
     } else {
-      k = (e / kTcT) * 2;
-      row = e % kTcT;
-      const int q0 = kind == kStageBPerm ? pv[k] : k;
-      const int q1 = kind == kStageBPerm ? pv[k + 1] : k + 1;
-      const size_t o0 = (size_t)q0 * kTcT + row, o1 = (size_t)q1 * kTcT + row;
-      re[0] = F[o0]; re[1] = F[o1];
-      im[0] = F[o0 + kTcT * kTcT]; im[1] = F[o1 + kTcT * kTcT];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int q = kind == kStageBPerm ? pv[k0 + t] : k0 + t;
+        const size_t o = (size_t)q * kTcT + row;
+        re[t] = F[o];
+        im[t] = F[o + kTcT * kTcT];
+      }
       if (kind == kStageBUpper) {
 #pragma unroll
-        for (int t = 0; t < 2; ++t)
-          if (k + t > row) re[t] = im[t] = 0.0f;
+        for (int t = 0; t < 8; ++t)
+          if (k0 + t > row) re[t] = im[t] = 0.0f;
       }
     }
-    __nv_bfloat162 plane[4];
+    uint32_t plane[4][4];
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      const __nv_bfloat16 rh = __float2bfloat16_rn(re[t]);
-      const __nv_bfloat16 rl = __float2bfloat16_rn(re[t] - __bfloat162float(rh));
-      const __nv_bfloat16 ih = __float2bfloat16_rn(im[t]);
-      const __nv_bfloat16 il = __float2bfloat16_rn(im[t] - __bfloat162float(ih));
-      if (t == 0) {
-        plane[0].x = rh; plane[1].x = rl; plane[2].x = ih; plane[3].x = il;
-      } else {
-        plane[0].y = rh; plane[1].y = rl; plane[2].y = ih; plane[3].y = il;
+    for (int t = 0; t < 8; t += 2) {
+      __nv_bfloat16 h[4][2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const __nv_bfloat16 rh = __float2bfloat16_rn(re[t + u]);
+        const __nv_bfloat16 ih = __float2bfloat16_rn(im[t + u]);
+        h[0][u] = rh;
+        h[1][u] = __float2bfloat16_rn(re[t + u] - __bfloat162float(rh));
+        h[2][u] = ih;
+        h[3][u] = __float2bfloat16_rn(im[t + u] - __bfloat162float(ih));
       }
+#pragma unroll
+      for (int pl = 0; pl < 4; ++pl) plane[pl][t / 2] = pack_bf16x2(h[pl][0], h[pl][1]);
     }
 #pragma unroll
     for (int pl = 0; pl < 4; ++pl)
-      *reinterpret_cast<__nv_bfloat162*>(out + staged_offset(row, k, pl)) = plane[pl];
+      *reinterpret_cast<uint4*>(out + staged_offset(row, k0, pl)) =
+          make_uint4(plane[pl][0], plane[pl][1], plane[pl][2], plane[pl][3]);
   }
 }
 

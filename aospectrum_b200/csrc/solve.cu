@@ -346,103 +346,139 @@ __global__ void shifted_residual_kernel(int64_t n, int nrhs, const int64_t* __re
   }
 }
 
-// Row-block version: rows [rb[b], rb[b+1]) (at most kResRows) share one
-// column pattern (the rows of one atom).  One CTA of kResWarps warps per
-// (block, 32-column strip, pencil); the warps split the block's columns.
-// Per chunk of 32 columns each lane forms A = H - z S in FP64 for one
-// column and every row of the block into shared memory (so A is formed
-// once, not once per lane); then every lane walks the chunk, loading each
-// x row once for all rows of the block.  Partial sums of the warps are
-// added in shared memory.
-constexpr int kResRows = 16;
+// Row-block kernels: rows [rb[b], rb[b+1]) share one column pattern (the
+// rows of one atom) and are stored one after another with equal lengths.
+// One CTA of kResWarps warps per (block, 32-column strip, pencil); the warps
+// split the block's nonzeros.  Per chunk of 32 nonzeros each lane forms the
+// FP64 matrix entries of one nonzero for every row of the block into shared
+// memory (so A is converted once, not once per lane); then every lane walks
+// the chunk, loading each x row once for all rows of the block, with the
+// loads of the next kXRows x rows issued before the products of the current
+// ones.  Partial sums of the warps are added in shared memory.
+//
+// kResidual: A = H(k_p) - z_p S(k_p) and y[p] = b[p] - A x[p] (FP64 residual
+// of every pencil of a batch).  Otherwise A = the single complex64 value
+// array and y = A x (the CISS products S Y, H B, S B).
 constexpr int kResWarps = 4;
+constexpr int kXRows = 4;
 
-__global__ void __launch_bounds__(kResWarps * 32) shifted_residual_blocks_kernel(
-    int64_t n_blocks, const int32_t* __restrict__ rb, int nrhs,
-    const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
-    const float2* __restrict__ hv, const float2* __restrict__ sv, int64_t nnz,
-    const int32_t* __restrict__ pencil_k, const double2* __restrict__ shifts,
-    const double2* __restrict__ b, int64_t b_stride, const double2* __restrict__ x,
-    double2* __restrict__ r, int64_t n) {
-  __shared__ double2 as[kResWarps][kResRows][32];
+struct RowBlockArgs {
+  int64_t n_blocks;
+  const int32_t* rb;
+  int ncols;
+  const int64_t* indptr;
+  const int32_t* indices;
+  const float2* hv;  // residual: H values [k][nnz]; product: A values [nnz]
+  const float2* sv;  // residual: S values [k][nnz] or null
+  int64_t nnz;
+  const int32_t* pencil_k;
+  const double2* shifts;
+  const double2* b;  // residual: b[p * b_stride + row * ldy + c]
+  int64_t b_stride;
+  const double2* x;  // x[p * x_stride + col * ldx + c]
+  int64_t ldx, x_stride;
+  double2* y;        // y[p * y_stride + row * ldy + c]
+  int64_t ldy, y_stride;
+};
+
+template <int R, bool kResidual>
+__global__ void __launch_bounds__(kResWarps * 32, 4) row_block_kernel(const RowBlockArgs a) {
+  __shared__ double2 as[kResWarps][R][32];
   __shared__ int32_t cs[kResWarps][32];
-  const int ncs = (nrhs + 31) / 32;
+  const int ncs = (a.ncols + 31) / 32;
   const int64_t blk = blockIdx.x / ncs;
   const int c = (int)(blockIdx.x % ncs) * 32 + (threadIdx.x & 31);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.y;
-  if (blk >= n_blocks) return;
-  const int r0 = rb[blk], nr = rb[blk + 1] - rb[blk];
-  const int64_t kp = pencil_k[p];
-  const double2 z = shifts[p];
-  const float2* h = hv + kp * nnz;
-  const float2* s = sv != nullptr ? sv + kp * nnz : nullptr;
-  const double2* xp = x + (size_t)p * n * nrhs;
-  const bool active = c < nrhs;
-  // rows of a block are consecutive with equal lengths: row q starts at
-  // base0 + q * len
-  const int64_t base0 = indptr[r0];
-  const int64_t len = indptr[r0 + 1] - base0;
+  if (blk >= a.n_blocks) return;
+  const int r0 = a.rb[blk], nr = a.rb[blk + 1] - a.rb[blk];
+  const int nq = nr < R ? nr : R;
+  const float2* h = a.hv;
+  const float2* s = nullptr;
+  double2 z = make_double2(0.0, 0.0);
+  if (kResidual) {
+    const int64_t kp = a.pencil_k[p];
+    z = a.shifts[p];
+    h = a.hv + kp * a.nnz;
+    s = a.sv != nullptr ? a.sv + kp * a.nnz : nullptr;
+  }
+  const double2* xp = a.x + (size_t)p * a.x_stride;
+  const bool active = c < a.ncols;
+  // row q of the block starts at base0 + q * len
+  const int64_t base0 = a.indptr[r0];
+  const int64_t len = a.indptr[r0 + 1] - base0;
   const int64_t per = (len + kResWarps - 1) / kResWarps;
   const int64_t w0 = (int64_t)warp * per;
   const int64_t w1 = w0 + per < len ? w0 + per : len;
-  double ar[kResRows], ai[kResRows];
+  double ar[R], ai[R];
 #pragma unroll
-  for (int q = 0; q < kResRows; ++q) {
+  for (int q = 0; q < R; ++q) {
     ar[q] = 0.0;
     ai[q] = 0.0;
   }
   for (int64_t e0 = w0; e0 < w1; e0 += 32) {
     const int cnt = (int)(w1 - e0 < 32 ? w1 - e0 : 32);
     if (lane < cnt) {
-      cs[warp][lane] = indices[base0 + e0 + lane];
+      cs[warp][lane] = a.indices[base0 + e0 + lane];
 #pragma unroll
-      for (int q = 0; q < kResRows; ++q) {
-        if (q < nr) {
+      for (int q = 0; q < R; ++q) {
+        double2 v = make_double2(0.0, 0.0);  // rows past the block add nothing
+        if (q < nq) {
           const int64_t at = base0 + (int64_t)q * len + e0 + lane;
           const float2 hh = h[at];
-          const float2 ss = s != nullptr ? s[at] : make_float2(0.f, 0.f);
-          as[warp][q][lane] = make_double2((double)hh.x - (z.x * ss.x - z.y * ss.y),
-                                           (double)hh.y - (z.x * ss.y + z.y * ss.x));
+          if (kResidual) {
+            const float2 ss = s != nullptr ? s[at] : make_float2(0.f, 0.f);
+            v = make_double2((double)hh.x - (z.x * ss.x - z.y * ss.y),
+                             (double)hh.y - (z.x * ss.y + z.y * ss.x));
+          } else {
+            v = make_double2((double)hh.x, (double)hh.y);
+          }
         }
+        as[warp][q][lane] = v;
       }
     }
     __syncwarp();
-    constexpr int U = 4;  // x rows in flight together
-    for (int j0 = 0; j0 < cnt; j0 += U) {
-      double2 xv[U];
+    double2 xa[kXRows], xb[kXRows];
+    auto load = [&](double2(&buf)[kXRows], int j) {
 #pragma unroll
-      for (int u = 0; u < U; ++u)
-        xv[u] = (j0 + u < cnt && active) ? xp[(size_t)cs[warp][j0 + u] * nrhs + c]
+      for (int u = 0; u < kXRows; ++u)
+        buf[u] = (j + u < cnt && active) ? xp[(size_t)cs[warp][j + u] * a.ldx + c]
                                          : make_double2(0.0, 0.0);
+    };
+    auto madd = [&](const double2(&buf)[kXRows], int j) {
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (j0 + u >= cnt) break;
+      for (int u = 0; u < kXRows; ++u) {
+        if (j + u >= cnt) break;
 #pragma unroll
-        for (int q = 0; q < kResRows; ++q) {
-          if (q < nr) {
-            const double2 a = as[warp][q][j0 + u];
-            ar[q] += a.x * xv[u].x - a.y * xv[u].y;
-            ai[q] += a.x * xv[u].y + a.y * xv[u].x;
-          }
+        for (int q = 0; q < R; ++q) {
+          const double2 m = as[warp][q][j + u];
+          ar[q] += m.x * buf[u].x - m.y * buf[u].y;
+          ai[q] += m.x * buf[u].y + m.y * buf[u].x;
         }
       }
+    };
+    load(xa, 0);
+    for (int j0 = 0; j0 < cnt; j0 += 2 * kXRows) {
+      load(xb, j0 + kXRows);
+      madd(xa, j0);
+      load(xa, j0 + 2 * kXRows);
+      madd(xb, j0 + kXRows);
     }
     __syncwarp();
   }
   // cross-warp sum: reuse `as` as [warp][row][lane]
   __syncthreads();
 #pragma unroll
-  for (int q = 0; q < kResRows; ++q)
-    if (q < nr) as[warp][q][lane] = make_double2(ar[q], ai[q]);
+  for (int q = 0; q < R; ++q) as[warp][q][lane] = make_double2(ar[q], ai[q]);
   __syncthreads();
   if (!active) return;
   for (int q = warp; q < nr; q += kResWarps) {
     const int64_t row = r0 + q;
-    if (q >= kResRows) {
-      // blocks longer than kResRows break the contract: poison those rows
-      r[((size_t)p * n + row) * nrhs + c] = make_double2(__longlong_as_double(0x7ff8000000000000ll),
-                                                         __longlong_as_double(0x7ff8000000000000ll));
+    double2* out = a.y + (size_t)p * a.y_stride + (size_t)row * a.ldy + c;
+    if (q >= R) {
+      // blocks longer than R break the launch contract: poison those rows
+      *out = make_double2(__longlong_as_double(0x7ff8000000000000ll),
+                          __longlong_as_double(0x7ff8000000000000ll));
       continue;
     }
     double sr = 0.0, si = 0.0;
@@ -451,9 +487,36 @@ __global__ void __launch_bounds__(kResWarps * 32) shifted_residual_blocks_kernel
       sr += as[w][q][lane].x;
       si += as[w][q][lane].y;
     }
-    const double2 bv = b[(size_t)p * b_stride + (size_t)row * nrhs + c];
-    r[((size_t)p * n + row) * nrhs + c] = make_double2(bv.x - sr, bv.y - si);
+    if (kResidual) {
+      const double2 bv = a.b[(size_t)p * a.b_stride + (size_t)row * a.ldy + c];
+      *out = make_double2(bv.x - sr, bv.y - si);
+    } else {
+      *out = make_double2(sr, si);
+    }
   }
+}
+
+// Launches row_block_kernel with the smallest row count R >= max_rows.
+template <bool kResidual>
+int launch_row_blocks(const RowBlockArgs& a, int max_rows, int np, cudaStream_t st, char* err,
+                      size_t cap) {
+  const int ncs = (a.ncols + 31) / 32;
+  if (a.n_blocks * ncs > INT32_MAX)
+    return set_error(err, cap, AOSB_ERR_SIZE, "too many row blocks");
+  if (max_rows < 1 || max_rows > 16)
+    return set_error(err, cap, AOSB_ERR_ARGUMENT, "max_block_rows must be in 1..16");
+  dim3 g((unsigned)(a.n_blocks * ncs), np);
+  const int th = kResWarps * 32;
+  if (max_rows <= 4)
+    row_block_kernel<4, kResidual><<<g, th, 0, st>>>(a);
+  else if (max_rows <= 8)
+    row_block_kernel<8, kResidual><<<g, th, 0, st>>>(a);
+  else if (max_rows <= 13)
+    row_block_kernel<13, kResidual><<<g, th, 0, st>>>(a);
+  else
+    row_block_kernel<16, kResidual><<<g, th, 0, st>>>(a);
+  count_launches(1);
+  return 0;
 }
 
 }  // namespace
@@ -640,34 +703,57 @@ int aosb_scatter_solution(const aosb_plan_t* P, int32_t np, int32_t nrhs,
 }
 
 int aosb_shifted_residual_blocks(int64_t n, int32_t nrhs, int32_t np, int64_t n_blocks,
-                                 const int32_t* row_blocks, const int64_t* indptr,
-                                 const int32_t* indices, const aosb_complex64* h_values,
-                                 const aosb_complex64* s_values, int64_t nnz,
-                                 const int32_t* pencil_k, const aosb_complex128* shifts,
-                                 const aosb_complex128* b, int64_t b_stride,
-                                 const aosb_complex128* x, aosb_complex128* r, void* stream,
-                                 char* err, size_t cap) {
+                                 const int32_t* row_blocks, int32_t max_block_rows,
+                                 const int64_t* indptr, const int32_t* indices,
+                                 const aosb_complex64* h_values, const aosb_complex64* s_values,
+                                 int64_t nnz, const int32_t* pencil_k,
+                                 const aosb_complex128* shifts, const aosb_complex128* b,
+                                 int64_t b_stride, const aosb_complex128* x, aosb_complex128* r,
+                                 void* stream, char* err, size_t cap) {
   if (row_blocks == nullptr || indptr == nullptr || indices == nullptr || h_values == nullptr ||
       pencil_k == nullptr || shifts == nullptr || b == nullptr || x == nullptr || r == nullptr)
     return aosb::set_error(err, cap, AOSB_ERR_NULL, "null argument");
   if (np <= 0 || np > 65535 || nrhs <= 0 || n <= 0 || n_blocks <= 0)
     return aosb::set_error(err, cap, AOSB_ERR_BATCH, "invalid batch");
-  const int ncs = (nrhs + 31) / 32;
-  if (n_blocks * ncs > INT32_MAX) return aosb::set_error(err, cap, AOSB_ERR_SIZE, "too many row blocks");
-  dim3 g((unsigned)(n_blocks * ncs), np);
+  aosb::RowBlockArgs a{n_blocks, row_blocks, nrhs, indptr, indices, (const float2*)h_values,
+                       (const float2*)s_values, nnz, pencil_k, (const double2*)shifts,
+                       (const double2*)b, b_stride, (const double2*)x, nrhs, n * nrhs,
+                       (double2*)r, nrhs, n * nrhs};
   cudaEvent_t ev[2];
   const bool timed = aosb::timing_begin((cudaStream_t)stream, ev);
-  aosb::shifted_residual_blocks_kernel<<<g, aosb::kResWarps * 32, 0, (cudaStream_t)stream>>>(
-      n_blocks, row_blocks, nrhs, indptr, indices, (const float2*)h_values,
-      (const float2*)s_values, nnz, pencil_k, (const double2*)shifts, (const double2*)b,
-      b_stride, (const double2*)x, (double2*)r, n);
-  aosb::count_launches(1);
+  int rc = aosb::launch_row_blocks<true>(a, max_block_rows, np, (cudaStream_t)stream, err, cap);
+  if (rc) return rc;
   // algorithmic: 8 FP64 flops per (nonzero, column, pencil); H and S values
   // once per k, x read and r written once per pencil
   if (timed)
     aosb::timing_end(aosb::kTimedResidual, (cudaStream_t)stream, ev, 8.0 * nnz * nrhs * np,
                      16.0 * nnz + (double)np * n * nrhs * 16.0 * 3.0);
   return aosb::launch_check(err, cap, "shifted_residual_blocks");
+}
+
+int aosb_spmm_blocks(int64_t n, int32_t ncols, int64_t n_blocks, const int32_t* row_blocks,
+                     int32_t max_block_rows, const int64_t* indptr, const int32_t* indices,
+                     const aosb_complex64* values, int64_t nnz, const aosb_complex128* x,
+                     int64_t ldx, aosb_complex128* y, int64_t ldy, void* stream, char* err,
+                     size_t cap) {
+  if (row_blocks == nullptr || indptr == nullptr || indices == nullptr || values == nullptr ||
+      x == nullptr || y == nullptr)
+    return aosb::set_error(err, cap, AOSB_ERR_NULL, "null argument");
+  if (n <= 0 || ncols <= 0 || n_blocks <= 0 || ldx < ncols || ldy < ncols)
+    return aosb::set_error(err, cap, AOSB_ERR_ARGUMENT, "invalid spmm shape");
+  aosb::RowBlockArgs a{n_blocks, row_blocks, ncols, indptr, indices, (const float2*)values,
+                       nullptr, nnz, nullptr, nullptr, nullptr, 0, (const double2*)x, ldx, 0,
+                       (double2*)y, ldy, 0};
+  cudaEvent_t ev[2];
+  const bool timed = aosb::timing_begin((cudaStream_t)stream, ev);
+  int rc = aosb::launch_row_blocks<false>(a, max_block_rows, 1, (cudaStream_t)stream, err, cap);
+  if (rc) return rc;
+  // algorithmic: 8 FP64 flops per (nonzero, column); A once, x read and y
+  // written once
+  if (timed)
+    aosb::timing_end(aosb::kTimedSpmm, (cudaStream_t)stream, ev, 8.0 * nnz * ncols,
+                     8.0 * nnz + (double)n * ncols * 32.0);
+  return aosb::launch_check(err, cap, "spmm_blocks");
 }
 
 int aosb_shifted_residual(int64_t n, int32_t nrhs, int32_t np, const int64_t* indptr,

@@ -325,6 +325,7 @@ class BundleResources:
                                  supervariables=supervariables, ordering=ordering,
                                  device=self.device, upload=False)
         self._rb = row_blocks(self.bloch.indptr, self.bloch.indices, starts=supervariables[:-1])
+        self.max_block_rows = int(np.diff(self._rb).max())
         self.row_blocks = None
         self.uploaded = False
 
@@ -371,6 +372,7 @@ class BandEngine:
             self.bloch = self.pattern = resources.bloch
             self.plan = resources.plan
             self.row_blocks = resources.row_blocks
+            self.max_block_rows = resources.max_block_rows
             self.pattern_seconds = self.analysis_seconds = 0.0
             self.tuning = None
             if self.settings.search_dimension >= self.n:
@@ -396,6 +398,7 @@ class BandEngine:
         rb = row_blocks(self.pattern.indptr, self.pattern.indices,
                         starts=None if supervariables is None else supervariables[:-1])
         self.row_blocks = torch.from_numpy(rb).to(self.device)
+        self.max_block_rows = int(np.diff(rb).max())
         t0 = perf_counter()
         use_tc = self.engine.precision == "mixed" and self.engine.tensor_cores
         tile = self.engine.tile or (128 if use_tc else choose_tile(self.n))
@@ -444,9 +447,10 @@ class BandEngine:
     def _spmm(self, values, x, y) -> None:
         """y = A x for one k (values [nnz] complex64)."""
         n, m = x.shape
-        native.call("aosb_spmm", n, m, self.pattern.d_indptr, self.pattern.d_indices,
-                    values.data_ptr(), x.data_ptr(), x.stride(0), y.data_ptr(), y.stride(0),
-                    self._stream())
+        native.call("aosb_spmm_blocks", n, m, self.row_blocks.numel() - 1,
+                    self.row_blocks.data_ptr(), self.max_block_rows, self.pattern.d_indptr,
+                    self.pattern.d_indices, values.data_ptr(), self.pattern.nnz, x.data_ptr(),
+                    x.stride(0), y.data_ptr(), y.stride(0), self._stream())
 
     def _gram(self, x, y):
         """x^H y (p x q) in FP64 on the device."""
@@ -700,7 +704,7 @@ class BandEngine:
         """FP64 r = b - (H - z S) x for every pencil of the batch."""
         if self.residual_kernel == "blocks":
             native.call("aosb_shifted_residual_blocks", n, L, np_, self.row_blocks.numel() - 1,
-                        self.row_blocks.data_ptr(), self.pattern.d_indptr,
+                        self.row_blocks.data_ptr(), self.max_block_rows, self.pattern.d_indptr,
                         self.pattern.d_indices, hvals.data_ptr(), svals.data_ptr(),
                         self.pattern.nnz, pk.data_ptr(), z.contiguous().data_ptr(),
                         b.data_ptr(), n * L, xn.data_ptr(), rr.data_ptr(), st)

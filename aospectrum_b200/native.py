@@ -134,9 +134,11 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_shifted_residual": (C.c_int, [c_i64, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp, c_i64,
                                         c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp,
                                         C.c_char_p, c_sz]),
-    "aosb_shifted_residual_blocks": (C.c_int, [c_i64, c_i32, c_i32, c_i64, c_vp, c_vp, c_vp,
-                                               c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_i64,
-                                               c_vp, c_vp, c_vp, C.c_char_p, c_sz]),
+    "aosb_shifted_residual_blocks": (C.c_int, [c_i64, c_i32, c_i32, c_i64, c_vp, c_i32, c_vp,
+                                               c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp,
+                                               c_i64, c_vp, c_vp, c_vp, C.c_char_p, c_sz]),
+    "aosb_spmm_blocks": (C.c_int, [c_i64, c_i32, c_i64, c_vp, c_i32, c_vp, c_vp, c_vp, c_i64,
+                                   c_vp, c_i64, c_vp, c_i64, c_vp, C.c_char_p, c_sz]),
     "aosb_spmm": (C.c_int, [c_i64, c_i32, c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_i64, c_vp,
                             C.c_char_p, c_sz]),
     "aosb_moments_accumulate": (C.c_int, [c_i64, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp,

@@ -20,8 +20,8 @@
  *   - aosb_plan_*, aosb_factor, aosb_solve and the IR helpers replace the
  *     cuDSS ANALYSIS / FACTORIZATION / SOLVE phases called from
  *     native/src/aospectrum_cudss_complex64_ubatch.c:446-600.
- *   - aosb_spmm, aosb_moments_accumulate, aosb_gram, aosb_dense_mul and
- *     aosb_column_norms replace the host numpy/scipy steps of
+ *   - aosb_spmm(_blocks), aosb_moments_accumulate, aosb_gram, aosb_dense_mul
+ *     and aosb_column_norms replace the host numpy/scipy steps of
  *     CudssCissSolver.solve_interval (src/aospectrum/ciss.py:284-372).
  */
 #ifndef AOSPECTRUM_B200_H
@@ -360,10 +360,12 @@ int aosb_shifted_residual(int64_t n, int32_t n_rhs, int32_t n_pencils,
 
 /* The same residual for patterns whose rows come in blocks with identical
  * column sets (the orbitals of one atom): row_blocks[n_blocks+1] (device)
- * are block start rows, each block at most 16 rows.  Each x row is read
- * once per block. */
+ * are block start rows, every block at most max_block_rows (1..16) rows;
+ * rows of a block longer than that come back NaN.  Each x row is read once
+ * per block. */
 int aosb_shifted_residual_blocks(int64_t n, int32_t n_rhs, int32_t n_pencils,
                                  int64_t n_blocks, const int32_t *row_blocks,
+                                 int32_t max_block_rows,
                                  const int64_t *indptr, const int32_t *indices,
                                  const aosb_complex64 *h_values,
                                  const aosb_complex64 *s_values, int64_t nnz,
@@ -381,6 +383,14 @@ int aosb_spmm(int64_t n, int32_t ncols, const int64_t *indptr,
               const int32_t *indices, const aosb_complex64 *values,
               const aosb_complex128 *x, int64_t ldx, aosb_complex128 *y,
               int64_t ldy, void *stream, char *err, size_t err_cap);
+/* y = A x on a row-blocked pattern (row_blocks and max_block_rows as for
+ * aosb_shifted_residual_blocks): each x row is read once per block. */
+int aosb_spmm_blocks(int64_t n, int32_t ncols, int64_t n_blocks,
+                     const int32_t *row_blocks, int32_t max_block_rows,
+                     const int64_t *indptr, const int32_t *indices,
+                     const aosb_complex64 *values, int64_t nnz,
+                     const aosb_complex128 *x, int64_t ldx, aosb_complex128 *y,
+                     int64_t ldy, void *stream, char *err, size_t err_cap);
 /* mom[:, m*L:(m+1)*L] += coef[m] * x for m < n_moments. */
 int aosb_moments_accumulate(int64_t n, int32_t n_rhs, int32_t n_moments,
                             const aosb_complex128 *x, const aosb_complex128 *coef,

@@ -370,8 +370,9 @@ def test_row_block_residual_matches_per_row(torch):
         native.call("aosb_shifted_residual", n, L, P, dev.d_indptr, dev.d_indices, h.data_ptr(),
                     s.data_ptr(), dev.nnz, pk.data_ptr(), z.data_ptr(), bb.data_ptr(), n * L,
                     x.data_ptr(), r1.data_ptr(), st)
+        max_rows = int(torch.diff(rb).max().item())
         native.call("aosb_shifted_residual_blocks", n, L, P, rb.numel() - 1, rb.data_ptr(),
-                    dev.d_indptr, dev.d_indices, h.data_ptr(), s.data_ptr(), dev.nnz,
+                    max_rows, dev.d_indptr, dev.d_indices, h.data_ptr(), s.data_ptr(), dev.nnz,
                     pk.data_ptr(), z.data_ptr(), bb.data_ptr(), n * L, x.data_ptr(),
                     r2.data_ptr(), st)
         torch.cuda.synchronize()
@@ -380,6 +381,51 @@ def test_row_block_residual_matches_per_row(torch):
     finally:
         dev.close()
         plan.close()
+
+
+@pytest.mark.parametrize("bundle_name,max_rows,ncols",
+                         [("small2d", None, 40), ("small2d", 16, 7), ("c1", None, 128),
+                          ("c1", 4, 33)])
+def test_row_block_spmm_matches_per_row(bundle_name, max_rows, ncols, torch):
+    """aosb_spmm_blocks == aosb_spmm (FP64 sums in another order) and the
+    complex128 product A x in scipy; blocks split to at most max_rows rows."""
+    import scipy.sparse as sp
+
+    from aospectrum_b200 import native
+    from aospectrum_b200.engine import BlochDevice, row_blocks
+
+    b = getattr(bundles, bundle_name)()
+    dv = torch.device("cuda", 0)
+    dev = BlochDevice(b, dv)
+    try:
+        h, _ = dev.apply(np.asarray([bundles.KPOINTS[1]]))
+        n = dev.n
+        rb_h = row_blocks(dev.indptr, dev.indices, max_rows=max_rows or 16,
+                          starts=np.asarray(b.basis.atom_offsets)[:-1])
+        rb = torch.from_numpy(rb_h).to(dv)
+        rows = int(np.diff(rb_h).max())
+        rng = np.random.default_rng(11)
+        ld = ncols + 3   # strided x and y
+        x = torch.tensor(rng.standard_normal((n, ld)) + 1j * rng.standard_normal((n, ld)),
+                         device=dv)
+        y1 = torch.zeros((n, ld), dtype=torch.complex128, device=dv)
+        y2 = torch.zeros_like(y1)
+        st = torch.cuda.current_stream().cuda_stream
+        native.call("aosb_spmm", n, ncols, dev.d_indptr, dev.d_indices, h.data_ptr(),
+                    x.data_ptr(), ld, y1.data_ptr(), ld, st)
+        native.call("aosb_spmm_blocks", n, ncols, rb.numel() - 1, rb.data_ptr(), rows,
+                    dev.d_indptr, dev.d_indices, h.data_ptr(), dev.nnz, x.data_ptr(), ld,
+                    y2.data_ptr(), ld, st)
+        torch.cuda.synchronize()
+        a, c = y1.cpu().numpy(), y2.cpu().numpy()
+        assert np.max(np.abs(a - c)) <= 1e-12 * np.max(np.abs(a))
+        assert np.all(c[:, ncols:] == 0)
+        m = sp.csr_matrix((h[0].cpu().numpy().astype(np.complex128), dev.indices, dev.indptr),
+                          shape=(n, n))
+        ref = m @ x.cpu().numpy()[:, :ncols]
+        assert np.max(np.abs(c[:, :ncols] - ref)) <= 1e-12 * np.max(np.abs(ref))
+    finally:
+        dev.close()
 
 
 @pytest.mark.parametrize("adjoint", [0, 1])
