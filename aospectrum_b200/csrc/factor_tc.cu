@@ -36,6 +36,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -561,6 +562,9 @@ static int factor_tensor_map(void* factor, int64_t rows, CUtensorMap* map, char*
   return encode_f32_2d(factor, kTcT, (uint64_t)rows, 32, 32, true, map, err, cap);
 }
 
+// SMs left to the lookahead side stream (0 = the default rule); process-wide.
+std::atomic<int> g_lookahead_sms{0};
+
 int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
   if (P->T != kTcT)
     return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "tensor-core path needs tile = 128");
@@ -597,7 +601,10 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   // products and staging run on a side stream on `reserve` SMs while the
   // rest of step k's Schur update runs on the others.
   const bool lookahead = tc_panels && sms >= 32;
-  const int reserve = lookahead ? std::min(std::max(np, 8), sms / 4) : 0;
+  const int chosen = g_lookahead_sms.load();
+  const int reserve = !lookahead ? 0
+                      : chosen > 0 ? std::min(chosen, sms / 2)
+                                   : std::min(std::max(np, 8), sms / 4);
   cudaStream_t side = nullptr;
   cudaEvent_t ev_cross = nullptr, ev_panel = nullptr;
   if (lookahead) {
@@ -805,3 +812,8 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
 }
 
 }  // namespace aosb
+
+extern "C" int32_t aosb_factor_set_lookahead_sms(int32_t sms) {
+  if (sms < 0) return -1;
+  return aosb::g_lookahead_sms.exchange(sms);
+}

@@ -124,6 +124,7 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_plan_destroy": (None, [c_vp]),
     "aosb_factor_bytes": (c_sz, [c_vp, c_i32]),
     "aosb_factor_workspace_bytes": (c_sz, [c_vp, c_i32, c_i32]),
+    "aosb_factor_set_lookahead_sms": (c_i32, [c_i32]),
     "aosb_factor": (C.c_int, [c_vp, C.POINTER(FactorArgs), C.c_char_p, c_sz]),
     "aosb_solve": (C.c_int, [c_vp, C.POINTER(SolveArgs), C.c_char_p, c_sz]),
     "aosb_solve_scratch_bytes": (c_sz, [c_vp, c_i32, c_i32]),

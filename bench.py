@@ -65,6 +65,8 @@ def parse() -> argparse.Namespace:
                     help="1: time candidate tile plans and k-point batches on the device first")
     ap.add_argument("--schur-depth", type=int, default=2, choices=(1, 2),
                     help="tile steps per tensor-core Schur pass (2 = K 256)")
+    ap.add_argument("--lookahead-sms", type=int, default=0,
+                    help="SMs left to the factorization's lookahead side stream (0 = default)")
     ap.add_argument("--tensor-core-solves", type=int, default=-1,
                     help="1/0: split-BF16 tensor-core solve updates on/off (-1 = engine default)")
     return ap.parse_args()
@@ -317,6 +319,8 @@ def main() -> None:
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=dev)
+    if args.lookahead_sms:
+        native.library().aosb_factor_set_lookahead_sms(args.lookahead_sms)
     w, kp = workload(args.workload)
     bundle = synth.generate_bundle(w.spec)
     interval = EnergyInterval(w.window_ev[0] - GUARD_EV, w.window_ev[1] + GUARD_EV)
@@ -473,6 +477,7 @@ def main() -> None:
                    else 0,
                    "tensor_core_solves": bool(eng.engine.tensor_core_solves),
                    "schur_depth": eng.engine.schur_depth,
+                   "lookahead_sms": args.lookahead_sms or "default",
                    "autotune": tuning,
                    "factorizations_per_step": stats.get("factorizations"),
                    "pencil_batch": stats.get("pencil_batch"),
