@@ -90,8 +90,8 @@ __global__ void __launch_bounds__(256) gram_partial_kernel(int64_t n, int p, int
       for (int j = 0; j < 4; ++j) {
         const double2 yv = ys[rr][tb + j];
         // conj(xv) * yv
-        acc[j].x += xv.x * yv.x + xv.y * yv.y;
-        acc[j].y += xv.x * yv.y - xv.y * yv.x;
+        acc[j].x = fma(xv.x, yv.x, fma(xv.y, yv.y, acc[j].x));
+        acc[j].y = fma(xv.x, yv.y, fma(-xv.y, yv.x, acc[j].y));
       }
     }
     __syncthreads();
@@ -156,8 +156,8 @@ __global__ void __launch_bounds__(256) dense_mul_kernel(int64_t n, int p, int r,
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           const double2 b = ts[kk][tc + 16 * j];
-          acc[i][j].x += a.x * b.x - a.y * b.y;
-          acc[i][j].y += a.x * b.y + a.y * b.x;
+          acc[i][j].x = fma(a.x, b.x, fma(-a.y, b.y, acc[i][j].x));
+          acc[i][j].y = fma(a.x, b.y, fma(a.y, b.x, acc[i][j].y));
         }
       }
     }

@@ -197,6 +197,7 @@ constexpr int kStagesP = 4;
 constexpr int kEpiWarps = 8;
 constexpr int kPThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemColsP = 512;
+constexpr int kItemRing = 8;  // > items the producer can run ahead of the epilogue (~4)
 
 struct PShared {
   alignas(1024) unsigned char a[kStagesP][kOperandSlabBytes];
@@ -207,6 +208,8 @@ struct PShared {
   uint64_t acc_empty[2];
   uint32_t tmem_base;
   int failed;
+  // claimed item of the producer's j-th item (j % kItemRing), -1 = no more
+  int items[8];
   // per epilogue warp: one 32 x 32 block of -acc (re, im planes), laid out
   // as the TMA 128-byte swizzle expects (row r at r * 128 bytes, 16-byte
   // chunk c of the row at chunk position c ^ (r % 8))
@@ -315,7 +318,8 @@ __device__ __forceinline__ int item_target(const ItemMap& m, int pair) {
 __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     const ItemMap map, int n_pencils, int64_t n_slots, const unsigned char* __restrict__ staging,
     const unsigned char* __restrict__ staging1, int64_t staging_pencil_stride,
-    int32_t* __restrict__ status, const __grid_constant__ CUtensorMap tmap_c) {
+    int32_t* __restrict__ status, int* __restrict__ claim,
+    const __grid_constant__ CUtensorMap tmap_c) {
   const int n_pairs = map.n_pairs;
   extern __shared__ unsigned char dyn[];
   PShared& sh = *reinterpret_cast<PShared*>(
@@ -349,7 +353,27 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
-      for (int it = blockIdx.x; it < total && !sh.failed; it += gridDim.x) {
+      for (int j = 0; !sh.failed; ++j) {
+        int it = blockIdx.x + j * (int)gridDim.x;
+        if (claim != nullptr) {
+          // dynamic: the item index reaches the MMA issuer and the epilogue
+          // through sh.items, published by this thread's arrive on full[]
+          it = atomicAdd(claim, 1);
+          if (it >= total) it = -1;
+          sh.items[j % kItemRing] = it;
+          if (it < 0) {
+            // stop token: one slab slot whose full[] completes without data
+            if (!mbar_wait(&sh.empty[stage], phase ^ 1)) {
+              sh.failed = 1;
+              atomicCAS(&status[0], 0, (int)AOSB_ERR_TIMEOUT);
+              break;
+            }
+            mbar_arrive(&sh.full[stage]);
+            break;
+          }
+        } else if (it >= total) {
+          break;
+        }
         const int p = it / n_pairs, pair = it % n_pairs;
         int ia[2], ib[2], bf[2];
         const int nh = item_halves(map, pair, ia, ib, bf);
@@ -378,20 +402,37 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
       const uint32_t lbo = (kTcT / 8) * 128, sbo = 128;
       int stage = 0, acc = 0;
       uint32_t phase = 0, acc_phase = 0;
-      for (int it = blockIdx.x; it < total && !sh.failed; it += gridDim.x) {
+      for (int j = 0; !sh.failed; ++j) {
+        int it = blockIdx.x + j * (int)gridDim.x;
+        if (claim == nullptr && it >= total) break;
+        if (!mbar_wait(&sh.acc_empty[acc], acc_phase ^ 1)) {
+          sh.failed = 1;
+          atomicCAS(&status[claim == nullptr ? it / n_pairs : 0], 0, (int)AOSB_ERR_TIMEOUT);
+          break;
+        }
+        bool first_waited = false;
+        if (claim != nullptr) {
+          // the item index is published with the item's first slab
+          if (!mbar_wait(&sh.full[stage], phase)) {
+            sh.failed = 1;
+            atomicCAS(&status[0], 0, (int)AOSB_ERR_TIMEOUT);
+            break;
+          }
+          it = *reinterpret_cast<volatile int*>(&sh.items[j % kItemRing]);
+          if (it < 0) {
+            mbar_arrive(&sh.acc_full[acc]);  // stop token for the epilogue
+            break;
+          }
+          first_waited = true;
+        }
         const int p = it / n_pairs;
         int ia[2], ib[2], bf[2];
         const int nslabs = item_halves(map, it % n_pairs, ia, ib, bf) * kSlabs;
-        if (!mbar_wait(&sh.acc_empty[acc], acc_phase ^ 1)) {
-          sh.failed = 1;
-          atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
-          break;
-        }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t re = tmem + (uint32_t)acc * 256, im = re + kTcT;
         bool ok = true;
         for (int s = 0; s < nslabs; ++s) {
-          if (!mbar_wait(&sh.full[stage], phase)) {
+          if (!(s == 0 && first_waited) && !mbar_wait(&sh.full[stage], phase)) {
             ok = false;
             break;
           }
@@ -444,18 +485,24 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     const float sgn = store ? 1.0f : -1.0f;  // store acc / add -acc
     int acc = 0;
     uint32_t acc_phase = 0;
-    for (int it = blockIdx.x; it < total; it += gridDim.x) {
-      const int p = it / n_pairs, pair = it % n_pairs;
-      // first row of the target tile's real plane in the [rows][128] view
-      const int64_t row0 = ((int64_t)p * n_slots + item_target(map, pair)) * (2 * kTcT);
+    for (int j = 0;; ++j) {
+      int it = blockIdx.x + j * (int)gridDim.x;
+      if (claim == nullptr && it >= total) break;
       const bool ready = __all_sync(0xffffffffu, mbar_wait(&sh.acc_full[acc], acc_phase) ? 1 : 0);
       if (!ready) {
         if (lane == 0) {
           sh.failed = 1;
-          atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
+          atomicCAS(&status[claim == nullptr ? it / n_pairs : 0], 0, (int)AOSB_ERR_TIMEOUT);
         }
         break;
       }
+      if (claim != nullptr) {
+        it = *reinterpret_cast<volatile int*>(&sh.items[j % kItemRing]);
+        if (it < 0) break;
+      }
+      const int p = it / n_pairs, pair = it % n_pairs;
+      // first row of the target tile's real plane in the [rows][128] view
+      const int64_t row0 = ((int64_t)p * n_slots + item_target(map, pair)) * (2 * kTcT);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t base = tmem + (uint32_t)acc * 256 + (uint32_t)half * 64 + lane_addr;
 #pragma unroll
@@ -525,10 +572,13 @@ static int64_t staged_tiles_per_pencil(const aosb_plan* P) {
 
 // Four staging buffers (tile step k uses buffer k % 4): with two-step
 // updates and lookahead, steps k + 2 and k + 3 are staged while the
-// two-step update of steps k and k + 1 still reads theirs.
+// two-step update of steps k and k + 1 still reads theirs.  After them, 256
+// bytes hold the item counter of the shared two-step updates.
+constexpr size_t kClaimBytes = 256;
 size_t factor_tc_workspace(const aosb_plan* P, int32_t n_pencils) {
   if (P->T != kTcT) return 0;
-  return 4 * (size_t)staged_tiles_per_pencil(P) * kStagedTileBytes * (size_t)n_pencils;
+  return 4 * (size_t)staged_tiles_per_pencil(P) * kStagedTileBytes * (size_t)n_pencils +
+         kClaimBytes;
 }
 
 // Side stream of a caller stream for the lookahead panels (created once,
@@ -639,7 +689,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
         a->pivots, stage_buf(k), pencil_stride);
     const ItemMap pm{kMapPanel, nL, nU, nL + nU, 0, 0, nullptr, lslot, uslot, nullptr};
     schur_tc_kernel<<<grid_for((int64_t)(nL + nU) * np, cap_ctas), kPThreads, smem, s>>>(
-        pm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, tmap_c);
+        pm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c);
     count_launches(2);
     return 0;
   };
@@ -662,7 +712,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr,
                      nullptr};
     schur_tc_kernel<<<grid_for((int64_t)n_pairs * np, cap_ctas), kPThreads, smem, s>>>(
-        sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, tmap_c);
+        sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c);
     count_launches(1);
   };
   // Schur update of step k (the pairs `kind` selects) on the caller stream,
@@ -676,7 +726,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr,
                      nullptr};
     schur_tc_kernel<<<grid_for(items, cap_ctas), kPThreads, smem, st>>>(
-        sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, tmap_c);
+        sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c);
     count_launches(1);
     if (timed)
       timing_end(kTimedSchur, st, ev, (double)items * 8.0 * kTcT * kTcT * kTcT,
@@ -695,8 +745,12 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     if (cross > 0) schur_on(k, kMapCross, a0, b0, cross, cap_ctas, s);
   };
   // two-step update of super-step ss (tile steps 2 ss, 2 ss + 1), the cross
-  // or the rest items, on the caller stream, timed
-  auto two_step = [&](int64_t ss, bool cross, int cap_ctas) {
+  // or the rest items, on stream s (timed); with `claim` the launch takes
+  // items from the shared counter instead of a fixed share
+  int* claim_counter = reinterpret_cast<int*>(staging + 4 * (int64_t)np * pencil_stride);
+  auto two_step = [&](int64_t ss, bool cross, int cap_ctas, cudaStream_t s = nullptr,
+                      int* claim = nullptr, bool count_work = true) {
+    if (s == nullptr) s = st;
     const std::vector<int64_t>& off = cross ? P->ss_cross_off : P->ss_rest_off;
     const std::vector<int32_t>& host = cross ? P->ss_cross : P->ss_rest;
     const int32_t* dev = cross ? P->d_ss_cross : P->d_ss_rest;
@@ -707,18 +761,21 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     for (int64_t i = off[ss]; i < off[ss + 1]; ++i)
       halves += (host[5 * i + 1] >= 0 ? 1 : 0) + (host[5 * i + 3] >= 0 ? 1 : 0);
     cudaEvent_t ev[2];
-    const bool timed = timing_begin(st, ev);
+    const bool timed = count_work && timing_begin(s, ev);
     const ItemMap lm{kMapList, 0, 0, (int)n, 0, 0, nullptr, nullptr, nullptr, dev + 5 * off[ss]};
-    schur_tc_kernel<<<grid_for(n * np, cap_ctas), kPThreads, smem, st>>>(
-        lm, np, P->n_slots, stage_buf(k0), stage_buf(k0 + 1), pencil_stride, a->status, tmap_c);
+    schur_tc_kernel<<<grid_for(n * np, cap_ctas), kPThreads, smem, s>>>(
+        lm, np, P->n_slots, stage_buf(k0), stage_buf(k0 + 1), pencil_stride, a->status, claim,
+        tmap_c);
     count_launches(1);
     // algorithmic bytes: every target read and written once, the staged L
-    // and U tiles of both steps read once
+    // and U tiles of both steps read once.  Of two launches sharing one
+    // counter, the main one is timed with all the work: the second joins
+    // later on other SMs and ends within about one item of the first.
     const double staged = (double)(P->lb_off[k0 + 1] - P->lb_off[k0] + P->ur_off[k0 + 1] -
                                    P->ur_off[k0] + P->lb_off[k0 + 2] - P->lb_off[k0 + 1] +
                                    P->ur_off[k0 + 2] - P->ur_off[k0 + 1]);
     if (timed)
-      timing_end(kTimedSchur, st, ev, halves * np * 8.0 * kTcT * kTcT * kTcT,
+      timing_end(kTimedSchur, s, ev, halves * np * 8.0 * kTcT * kTcT * kTcT,
                  (double)n * np * 2.0 * 2 * kTcT * kTcT * sizeof(float) +
                      staged * np * kStagedTileBytes);
   };
@@ -744,6 +801,10 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
       const int64_t k2 = 2 * ss + 2, k3 = 2 * ss + 3;
       two_step(ss, true, sms);
       if (k2 < nb) {
+        // the rest items are shared through a counter: the main launch on
+        // sms - reserve SMs starts at once, a second launch on the reserved
+        // SMs joins it once the side stream's panel work is done
+        AOSB_CUDA_TRY(cudaMemsetAsync(claim_counter, 0, sizeof(int), st), err, cap);
         AOSB_CUDA_TRY(cudaEventRecord(ev_cross, st), err, cap);
         AOSB_CUDA_TRY(cudaStreamWaitEvent(side, ev_cross, 0), err, cap);
         if (int rc = panels(k2, side, reserve)) return rc;
@@ -753,8 +814,9 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
           if (int rc = panels(k3, side, reserve)) return rc;
           stage_schur(k3, side);
         }
+        two_step(ss, false, reserve, side, claim_counter, false);
         AOSB_CUDA_TRY(cudaEventRecord(ev_panel, side), err, cap);
-        two_step(ss, false, sms - reserve);
+        two_step(ss, false, sms - reserve, st, claim_counter, true);
         AOSB_CUDA_TRY(cudaStreamWaitEvent(st, ev_panel, 0), err, cap);
       } else {
         two_step(ss, false, sms);

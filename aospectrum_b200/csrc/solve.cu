@@ -348,8 +348,8 @@ __global__ void shifted_residual_kernel(int64_t n, int nrhs, const int64_t* __re
 
 // Row-block kernels: rows [rb[b], rb[b+1]) share one column pattern (the
 // rows of one atom) and are stored one after another with equal lengths.
-// One CTA of kResWarps warps per (block, 32-column strip, pencil); the warps
-// split the block's nonzeros.  Per chunk of 32 nonzeros each lane forms the
+// One CTA of kResWarps warps per (block, 32-column strip, pencil), pencils
+// fastest; the warps split the block's nonzeros.  Per chunk of 32 nonzeros each lane forms the
 // FP64 matrix entries of one nonzero for every row of the block into shared
 // memory (so A is converted once, not once per lane); then every lane walks
 // the chunk, loading each x row once for all rows of the block, with the
@@ -363,6 +363,7 @@ constexpr int kResWarps = 4;
 constexpr int kXRows = 4;
 
 struct RowBlockArgs {
+  int np;  // pencils (1 for the product)
   int64_t n_blocks;
   const int32_t* rb;
   int ncols;
@@ -385,11 +386,14 @@ template <int R, bool kResidual>
 __global__ void __launch_bounds__(kResWarps * 32, 4) row_block_kernel(const RowBlockArgs a) {
   __shared__ double2 as[kResWarps][R][32];
   __shared__ int32_t cs[kResWarps][32];
+  // CTA index = (block, strip) * np + pencil: the CTAs of all pencils of one
+  // row block run together and share its H, S values in L2
   const int ncs = (a.ncols + 31) / 32;
-  const int64_t blk = blockIdx.x / ncs;
-  const int c = (int)(blockIdx.x % ncs) * 32 + (threadIdx.x & 31);
+  const int p = (int)(blockIdx.x % a.np);
+  const int64_t bs = blockIdx.x / a.np;
+  const int64_t blk = bs / ncs;
+  const int c = (int)(bs % ncs) * 32 + (threadIdx.x & 31);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p = blockIdx.y;
   if (blk >= a.n_blocks) return;
   const int r0 = a.rb[blk], nr = a.rb[blk + 1] - a.rb[blk];
   const int nq = nr < R ? nr : R;
@@ -452,8 +456,11 @@ __global__ void __launch_bounds__(kResWarps * 32, 4) row_block_kernel(const RowB
 #pragma unroll
         for (int q = 0; q < R; ++q) {
           const double2 m = as[warp][q][j + u];
-          ar[q] += m.x * buf[u].x - m.y * buf[u].y;
-          ai[q] += m.x * buf[u].y + m.y * buf[u].x;
+          // four FMAs per complex product (no separate multiply and add)
+          ar[q] = fma(m.x, buf[u].x, ar[q]);
+          ar[q] = fma(-m.y, buf[u].y, ar[q]);
+          ai[q] = fma(m.x, buf[u].y, ai[q]);
+          ai[q] = fma(m.y, buf[u].x, ai[q]);
         }
       }
     };
@@ -501,11 +508,12 @@ template <bool kResidual>
 int launch_row_blocks(const RowBlockArgs& a, int max_rows, int np, cudaStream_t st, char* err,
                       size_t cap) {
   const int ncs = (a.ncols + 31) / 32;
-  if (a.n_blocks * ncs > INT32_MAX)
-    return set_error(err, cap, AOSB_ERR_SIZE, "too many row blocks");
+  if (a.n_blocks * ncs * np > INT32_MAX)
+    return set_error(err, cap, AOSB_ERR_SIZE, "too many row blocks x pencils");
   if (max_rows < 1 || max_rows > 16)
     return set_error(err, cap, AOSB_ERR_ARGUMENT, "max_block_rows must be in 1..16");
-  dim3 g((unsigned)(a.n_blocks * ncs), np);
+  if (a.np != np) return set_error(err, cap, AOSB_ERR_ARGUMENT, "pencil count mismatch");
+  dim3 g((unsigned)(a.n_blocks * ncs * np));
   const int th = kResWarps * 32;
   if (max_rows <= 4)
     row_block_kernel<4, kResidual><<<g, th, 0, st>>>(a);
@@ -715,7 +723,7 @@ int aosb_shifted_residual_blocks(int64_t n, int32_t nrhs, int32_t np, int64_t n_
     return aosb::set_error(err, cap, AOSB_ERR_NULL, "null argument");
   if (np <= 0 || np > 65535 || nrhs <= 0 || n <= 0 || n_blocks <= 0)
     return aosb::set_error(err, cap, AOSB_ERR_BATCH, "invalid batch");
-  aosb::RowBlockArgs a{n_blocks, row_blocks, nrhs, indptr, indices, (const float2*)h_values,
+  aosb::RowBlockArgs a{np, n_blocks, row_blocks, nrhs, indptr, indices, (const float2*)h_values,
                        (const float2*)s_values, nnz, pencil_k, (const double2*)shifts,
                        (const double2*)b, b_stride, (const double2*)x, nrhs, n * nrhs,
                        (double2*)r, nrhs, n * nrhs};
@@ -741,7 +749,7 @@ int aosb_spmm_blocks(int64_t n, int32_t ncols, int64_t n_blocks, const int32_t* 
     return aosb::set_error(err, cap, AOSB_ERR_NULL, "null argument");
   if (n <= 0 || ncols <= 0 || n_blocks <= 0 || ldx < ncols || ldy < ncols)
     return aosb::set_error(err, cap, AOSB_ERR_ARGUMENT, "invalid spmm shape");
-  aosb::RowBlockArgs a{n_blocks, row_blocks, ncols, indptr, indices, (const float2*)values,
+  aosb::RowBlockArgs a{1, n_blocks, row_blocks, ncols, indptr, indices, (const float2*)values,
                        nullptr, nnz, nullptr, nullptr, nullptr, 0, (const double2*)x, ldx, 0,
                        (double2*)y, ldy, 0};
   cudaEvent_t ev[2];
