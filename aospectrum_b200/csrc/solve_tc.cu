@@ -32,6 +32,8 @@
 
 #include <cuda_bf16.h>
 
+#include <atomic>
+
 namespace aosb {
 namespace {
 
@@ -41,8 +43,6 @@ constexpr int kT = 128;
 constexpr int kNS = kSolveNS;              // RHS columns per item (32)
 constexpr int kSK = 16;                    // K per slab
 constexpr int kSlabsS = kT / kSK;          // 8
-constexpr int kRawStages = 4;              // FP32 slab ring
-constexpr int kAStages = 3;                // BF16 A slab ring
 constexpr int kConvWarps = 4, kEpiWarps = 4;
 constexpr int kConvWarp0 = 2, kEpiWarp0 = kConvWarp0 + kConvWarps;  // 2, 6
 constexpr int kSThreads = (kEpiWarp0 + kEpiWarps) * 32;              // 320
@@ -55,17 +55,34 @@ constexpr int kCopyCtas = 4;
 
 enum SolveOp { kOpPlain = 0, kOpConjT = 1 };
 
+// Ring depths and CTAs per SM.  Form 1: one CTA per SM with deep rings
+// (FP32 slabs 4, BF16 slabs 3, Y strips 2, two epilogue boxes per warp;
+// 208 KB).  Form 2: two CTAs per SM with shallow rings (2, 1, 1, one box per
+// warp; 96 KB), so that one CTA's waits overlap the other's work.
+template <int CTAS>
+struct SolveCfg;
+template <>
+struct SolveCfg<1> {
+  static constexpr int kRawStages = 4, kAStages = 3, kBStages = 2, kEpBoxes = 2;
+};
+template <>
+struct SolveCfg<2> {
+  static constexpr int kRawStages = 2, kAStages = 1, kBStages = 1, kEpBoxes = 1;
+};
+
+template <int CTAS>
 struct SShared {
+  using C = SolveCfg<CTAS>;
   // per epilogue warp: its 32 rows x 32 complex of -acc as two 32 x 32 FP32
-  // boxes (complex columns 0-15 and 16-31, re/im interleaved), laid out as
-  // the TMA 128-byte swizzle expects
-  alignas(1024) float ep[kEpiWarps][2][32 * 32];       // 32 KB
-  alignas(128) float raw[kRawStages][2][kRawPlane];   // 64 KB
-  alignas(128) unsigned char a[kAStages][kASlab];      // 48 KB
-  alignas(128) unsigned char b[2][kSolveBBytes];       // 64 KB
-  uint64_t raw_full[kRawStages], raw_empty[kRawStages];
-  uint64_t a_full[kAStages], a_empty[kAStages];
-  uint64_t b_full[2], b_empty[2];
+  // boxes (complex columns 0-15 and 16-31, re/im interleaved; with one box
+  // the halves take turns), laid out as the TMA 128-byte swizzle expects
+  alignas(1024) float ep[kEpiWarps][C::kEpBoxes][32 * 32];
+  alignas(128) float raw[C::kRawStages][2][kRawPlane];
+  alignas(128) unsigned char a[C::kAStages][kASlab];
+  alignas(128) unsigned char b[C::kBStages][kSolveBBytes];
+  uint64_t raw_full[C::kRawStages], raw_empty[C::kRawStages];
+  uint64_t a_full[C::kAStages], a_empty[C::kAStages];
+  uint64_t b_full[C::kBStages], b_empty[C::kBStages];
   uint64_t acc_full[2], acc_empty[2];
   uint32_t tmem_base;
   int failed;
@@ -99,13 +116,14 @@ __device__ __forceinline__ ItemOf item_of(int it, int n_items, int strips) {
   return r;
 }
 
-__device__ __forceinline__ void fail(SShared& sh, int32_t* status, int p) {
+template <typename SH>
+__device__ __forceinline__ void fail(SH& sh, int32_t* status, int p) {
   sh.failed = 1;
   atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
 }
 
-template <int OP>
-__global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
+template <int OP, int CTAS>
+__global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
     int k, int n_items, int nrhs, int n_pencils, int64_t n_pad, const int32_t* __restrict__ tiles,
     const int32_t* __restrict__ slots, int64_t n_slots, float2* __restrict__ work,
     const float2* __restrict__ ytmp, const unsigned char* __restrict__ ystaged,
@@ -125,8 +143,10 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
     }
     return;
   }
+  using C = SolveCfg<CTAS>;
+  constexpr int kRawStages = C::kRawStages, kAStages = C::kAStages, kBStages = C::kBStages;
   extern __shared__ unsigned char dyn[];
-  SShared& sh = *reinterpret_cast<SShared*>(
+  SShared<CTAS>& sh = *reinterpret_cast<SShared<CTAS>*>(
       (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if (threadIdx.x == 0) {
@@ -138,9 +158,11 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
       mbar_init(&sh.a_full[s], kConvWarps);
       mbar_init(&sh.a_empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < kBStages; ++b) {
       mbar_init(&sh.b_full[b], 1);
       mbar_init(&sh.b_empty[b], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
       mbar_init(&sh.acc_full[b], 1);
       mbar_init(&sh.acc_empty[b], kEpiWarps);
     }
@@ -165,8 +187,8 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
       int j = 0;  // item counter
       for (int it = blockIdx.x; it < total && !sh.failed; it += work_ctas, ++j) {
         const ItemOf w = item_of(it, n_items, strips);
-        const int bb = j & 1;
-        if (!mbar_wait(&sh.b_empty[bb], (uint32_t)(((j >> 1) & 1) ^ 1))) { fail(sh, status, w.p); break; }
+        const int bb = j % kBStages;
+        if (!mbar_wait(&sh.b_empty[bb], (uint32_t)(((j / kBStages) & 1) ^ 1))) { fail(sh, status, w.p); break; }
         mbar_expect_tx(&sh.b_full[bb], kSolveBBytes);
         bulk_g2s(sh.b[bb], ystaged + ((size_t)w.p * strips + w.strip) * kSolveBBytes,
                  kSolveBBytes, &sh.b_full[bb]);
@@ -200,9 +222,9 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
         const int ncols = nrhs - w.strip * kNS < kNS ? nrhs - w.strip * kNS : kNS;
         const int n16 = (ncols + 15) & ~15;
         const uint32_t id_pos = umma_idesc_mn(kT, n16, false), id_neg = umma_idesc_mn(kT, n16, true);
-        const int acc = j & 1, bb = j & 1;
+        const int acc = j & 1, bb = j % kBStages;
         if (!mbar_wait(&sh.acc_empty[acc], (uint32_t)(((j >> 1) & 1) ^ 1)) ||
-            !mbar_wait(&sh.b_full[bb], (uint32_t)((j >> 1) & 1))) {
+            !mbar_wait(&sh.b_full[bb], (uint32_t)((j / kBStages) & 1))) {
           fail(sh, status, w.p);
           break;
         }
@@ -328,12 +350,12 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh.acc_empty[acc]);
       const int64_t xrow = (int64_t)w.p * n_pad + (int64_t)tiles[w.tile_idx] * kT;
-      if (x_tma) {
+      if (x_tma && C::kEpBoxes == 2) {
         if (lane == 0) bulk_wait_read_all();   // the boxes' previous reduce has read them
         __syncwarp();
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          float* box = sh.ep[ew][h];
+          float* box = sh.ep[ew][h % C::kEpBoxes];
           // 16 complex = 32 floats = 8 chunks of 16 bytes: (re, im, re, im)
 #pragma unroll
           for (int c = 0; c < 8; ++c)
@@ -345,8 +367,28 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
         if (lane == 0) {
           const int y = (int)(xrow + quarter * 32);
           tma_reduce_add_2d(&xmap, sh.ep[ew][0], 2 * c0, y);
-          if (ncols > 16) tma_reduce_add_2d(&xmap, sh.ep[ew][1], 2 * c0 + 32, y);
+          if (ncols > 16) tma_reduce_add_2d(&xmap, sh.ep[ew][1 % C::kEpBoxes], 2 * c0 + 32, y);
           bulk_commit();
+        }
+      } else if (x_tma) {
+        // one box per warp: each half waits until the box's previous reduce
+        // has read it
+        float* box = sh.ep[ew][0];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (h == 1 && ncols <= 16) break;
+          if (lane == 0) bulk_wait_read_all();
+          __syncwarp();
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            *reinterpret_cast<float4*>(box + lane * 32 + ((c ^ sw) * 4)) =
+                make_float4(-vr[h][2 * c], -vi[h][2 * c], -vr[h][2 * c + 1], -vi[h][2 * c + 1]);
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) {
+            tma_reduce_add_2d(&xmap, box, 2 * c0 + 32 * h, (int)(xrow + quarter * 32));
+            bulk_commit();
+          }
         }
       } else {
         float2* xr = work + (size_t)(xrow + row) * nrhs + c0;
@@ -383,26 +425,50 @@ __global__ void __launch_bounds__(kSThreads, 1) solve_tc_kernel(
 
 }  // namespace
 
-size_t solve_tc_smem() { return sizeof(SShared) + 1024; }
+template <int CTAS>
+size_t solve_tc_smem() { return sizeof(SShared<CTAS>) + 1024; }
+static_assert(sizeof(SShared<1>) + 1024 <= 232448, "shared memory budget");
+// two CTAs and their 1 KB system reservations in the SM's 228 KB
+static_assert(2 * (sizeof(SShared<2>) + 1024 + 1024) <= 233472, "two CTAs per SM");
+
+// CTAs per SM of the tensor-core solve update (1 or 2); process-wide.
+std::atomic<int> g_solve_ctas{1};
+
+template <int OP, int CTAS>
+int solve_tc_launch(int k, int n, const int32_t* dtiles, const int32_t* dslots, int np, int nrhs,
+                    const aosb_plan* P, float2* work, const float2* ytmp,
+                    const unsigned char* ystaged, int32_t* status, const CUtensorMap& fmap,
+                    const CUtensorMap& xmap, int x_tma, int sms, cudaStream_t st, char* err,
+                    size_t cap) {
+  static bool attr_done = false;
+  const size_t smem = solve_tc_smem<CTAS>();
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(solve_tc_kernel<OP, CTAS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && CTAS > 1)
+      e = cudaFuncSetAttribute(solve_tc_kernel<OP, CTAS>,
+                               cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess)
+      return set_error(err, cap, AOSB_ERR_CUDA, "solve_tc attributes: %s", cudaGetErrorString(e));
+    attr_done = true;
+  }
+  const int strips = (nrhs + kNS - 1) / kNS;
+  const int64_t items = (int64_t)n * strips * np;
+  const int64_t slots = (int64_t)CTAS * sms;
+  const int work_ctas = (int)(items < slots ? items : slots);
+  dim3 g((unsigned)(work_ctas + kCopyCtas));
+  solve_tc_kernel<OP, CTAS><<<g, kSThreads, smem, st>>>(k, n, nrhs, np, P->n_pad, dtiles, dslots,
+                                                        P->n_slots, work, ytmp, ystaged, status,
+                                                        fmap, xmap, x_tma);
+  count_launches(1);
+  return 0;
+}
 
 // Launch the tensor-core update of step k for n tiles (device lists).
 int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, int op,
                     int np, int nrhs, const aosb_plan* P, const float* factor, float2* work,
                     const float2* ytmp, const unsigned char* ystaged, int32_t* status,
                     cudaStream_t st, char* err, size_t cap) {
-  static bool attr_done[2] = {false, false};
-  const size_t smem = solve_tc_smem();
-  static_assert(sizeof(SShared) + 1024 <= 232448, "shared memory budget");
-  if (!attr_done[op]) {
-    cudaError_t e = op == kOpPlain
-                        ? cudaFuncSetAttribute(solve_tc_kernel<kOpPlain>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                        : cudaFuncSetAttribute(solve_tc_kernel<kOpConjT>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess)
-      return set_error(err, cap, AOSB_ERR_CUDA, "solve_tc smem attribute: %s", cudaGetErrorString(e));
-    attr_done[op] = true;
-  }
   // the factor as [rows][128] FP32; plain slabs are {16, 128} boxes,
   // adjoint slabs {128, 16}
   CUtensorMap fmap;
@@ -426,20 +492,21 @@ int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
   int device = 0, sms = 148;
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  const int strips = (nrhs + kNS - 1) / kNS;
-  const int64_t items = (int64_t)n * strips * np;
-  const int work_ctas = (int)(items < sms ? items : sms);
-  dim3 g((unsigned)(work_ctas + kCopyCtas));
+  const bool two = g_solve_ctas.load() == 2;
   if (op == kOpPlain)
-    solve_tc_kernel<kOpPlain><<<g, kSThreads, smem, st>>>(k, n, nrhs, np, P->n_pad, dtiles, dslots,
-                                                          P->n_slots, work, ytmp, ystaged, status,
-                                                          fmap, xmap, x_tma);
-  else
-    solve_tc_kernel<kOpConjT><<<g, kSThreads, smem, st>>>(k, n, nrhs, np, P->n_pad, dtiles, dslots,
-                                                          P->n_slots, work, ytmp, ystaged, status,
-                                                          fmap, xmap, x_tma);
-  count_launches(1);
-  return 0;
+    return two ? solve_tc_launch<kOpPlain, 2>(k, n, dtiles, dslots, np, nrhs, P, work, ytmp,
+                                              ystaged, status, fmap, xmap, x_tma, sms, st, err, cap)
+               : solve_tc_launch<kOpPlain, 1>(k, n, dtiles, dslots, np, nrhs, P, work, ytmp,
+                                              ystaged, status, fmap, xmap, x_tma, sms, st, err, cap);
+  return two ? solve_tc_launch<kOpConjT, 2>(k, n, dtiles, dslots, np, nrhs, P, work, ytmp, ystaged,
+                                            status, fmap, xmap, x_tma, sms, st, err, cap)
+             : solve_tc_launch<kOpConjT, 1>(k, n, dtiles, dslots, np, nrhs, P, work, ytmp, ystaged,
+                                            status, fmap, xmap, x_tma, sms, st, err, cap);
 }
 
 }  // namespace aosb
+
+extern "C" int32_t aosb_solve_set_ctas_per_sm(int32_t ctas) {
+  if (ctas < 0 || ctas > 2) return -1;
+  return aosb::g_solve_ctas.exchange(ctas == 0 ? 1 : ctas);
+}

@@ -125,6 +125,7 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_factor_bytes": (c_sz, [c_vp, c_i32]),
     "aosb_factor_workspace_bytes": (c_sz, [c_vp, c_i32, c_i32]),
     "aosb_factor_set_lookahead_sms": (c_i32, [c_i32]),
+    "aosb_solve_set_ctas_per_sm": (c_i32, [c_i32]),
     "aosb_factor": (C.c_int, [c_vp, C.POINTER(FactorArgs), C.c_char_p, c_sz]),
     "aosb_solve": (C.c_int, [c_vp, C.POINTER(SolveArgs), C.c_char_p, c_sz]),
     "aosb_solve_scratch_bytes": (c_sz, [c_vp, c_i32, c_i32]),

@@ -67,6 +67,8 @@ def parse() -> argparse.Namespace:
                     help="tile steps per tensor-core Schur pass (2 = K 256)")
     ap.add_argument("--lookahead-sms", type=int, default=0,
                     help="SMs left to the factorization's lookahead side stream (0 = default)")
+    ap.add_argument("--solve-ctas", type=int, default=0, choices=(0, 1, 2),
+                    help="CTAs per SM of the tensor-core solve update (0 = default)")
     ap.add_argument("--tensor-core-solves", type=int, default=-1,
                     help="1/0: split-BF16 tensor-core solve updates on/off (-1 = engine default)")
     return ap.parse_args()
@@ -321,6 +323,8 @@ def main() -> None:
                                 device_id=dev)
     if args.lookahead_sms:
         native.library().aosb_factor_set_lookahead_sms(args.lookahead_sms)
+    if args.solve_ctas:
+        native.library().aosb_solve_set_ctas_per_sm(args.solve_ctas)
     w, kp = workload(args.workload)
     bundle = synth.generate_bundle(w.spec)
     interval = EnergyInterval(w.window_ev[0] - GUARD_EV, w.window_ev[1] + GUARD_EV)
@@ -478,6 +482,7 @@ def main() -> None:
                    "tensor_core_solves": bool(eng.engine.tensor_core_solves),
                    "schur_depth": eng.engine.schur_depth,
                    "lookahead_sms": args.lookahead_sms or "default",
+                   "solve_ctas_per_sm": args.solve_ctas or "default",
                    "autotune": tuning,
                    "factorizations_per_step": stats.get("factorizations"),
                    "pencil_batch": stats.get("pencil_batch"),

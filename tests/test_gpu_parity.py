@@ -450,6 +450,34 @@ def test_graph_replayed_solve_equals_direct(adjoint, torch):
         plan.close()
 
 
+@pytest.mark.parametrize("adjoint,L", [(0, 32), (1, 32), (0, 40), (1, 40)])
+def test_tc_solve_two_ctas_per_sm_equals_one(adjoint, L, torch):
+    """The tensor-core solve update with two CTAs per SM (shallow rings, one
+    epilogue box per warp) gives the one-CTA result bit for bit (each X tile
+    gets one reduce-add per step in both forms); L = 40 adds an 8-column
+    strip."""
+    from aospectrum_b200 import native
+
+    b = bundles.c1()
+    dev, plan, h, s = _pencil_case(b, bundles.KPOINTS[1], torch, 128, "natural")
+    lib = native.library()
+    try:
+        rng = np.random.default_rng(8)
+        rhs = (rng.standard_normal((dev.n, L)) + 1j * rng.standard_normal((dev.n, L)))
+        shifts = [-2.6 + 0.02j, -1.0 + 0.3j, -2.2 + 0.1j]
+        kw = dict(precision=native.PRECISION_BF16X3, adjoint=adjoint, steps=1,
+                  flags=native.SOLVE_TENSOR_CORES)
+        lib.aosb_solve_set_ctas_per_sm(1)
+        one = _factor_solve(dev, plan, h, s, shifts, rhs, torch, **kw)
+        lib.aosb_solve_set_ctas_per_sm(2)
+        two = _factor_solve(dev, plan, h, s, shifts, rhs, torch, **kw)
+        assert np.array_equal(one, two)
+    finally:
+        lib.aosb_solve_set_ctas_per_sm(0)
+        dev.close()
+        plan.close()
+
+
 def test_two_step_factor_matches_one_step(torch):
     """Two-step (K = 256) Schur updates give the factor of the one-step
     updates up to split-BF16 rounding (same pivots on this pencil)."""
