@@ -431,8 +431,9 @@ static_assert(sizeof(SShared<1>) + 1024 <= 232448, "shared memory budget");
 // two CTAs and their 1 KB system reservations in the SM's 228 KB
 static_assert(2 * (sizeof(SShared<2>) + 1024 + 1024) <= 233472, "two CTAs per SM");
 
-// CTAs per SM of the tensor-core solve update (1 or 2); process-wide.
-std::atomic<int> g_solve_ctas{1};
+// CTAs per SM of the tensor-core solve update (1 or 2; 2 measured ~5 %
+// faster per launch on c2); process-wide.
+std::atomic<int> g_solve_ctas{2};
 
 template <int OP, int CTAS>
 int solve_tc_launch(int k, int n, const int32_t* dtiles, const int32_t* dslots, int np, int nrhs,
@@ -508,5 +509,5 @@ int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
 
 extern "C" int32_t aosb_solve_set_ctas_per_sm(int32_t ctas) {
   if (ctas < 0 || ctas > 2) return -1;
-  return aosb::g_solve_ctas.exchange(ctas == 0 ? 1 : ctas);
+  return aosb::g_solve_ctas.exchange(ctas == 0 ? 2 : ctas);
 }

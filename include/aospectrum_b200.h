@@ -345,9 +345,9 @@ int aosb_solve(const aosb_plan_t *plan, const aosb_solve_args_v1 *args,
 int aosb_solve_check(const aosb_plan_t *plan, const aosb_solve_args_v1 *args,
                      char *err, size_t err_cap);
 /* CTAs per SM of the tensor-core solve update (AOSB_SOLVE_TENSOR_CORES):
- * 1 (default: deep slab and RHS rings, 208 KB of shared memory) or 2
- * (shallow rings, 96 KB each, so one CTA's waits overlap the other's work);
- * 0 restores the default.  Process-wide; graphs captured before a change
+ * 1 (deep slab and RHS rings, 208 KB of shared memory) or 2 (default:
+ * shallow rings, 96 KB each, so one CTA's waits overlap the other's work;
+ * bit-identical results); 0 restores the default.  Process-wide; graphs captured before a change
  * keep the form they captured.  Returns the previous setting (-1 for values
  * outside 0..2).  No counterpart in the reference (cuDSS schedules
  * internally). */
