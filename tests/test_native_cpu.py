@@ -249,3 +249,39 @@ def test_shift_session_argument_checks():
     s.close()
     with pytest.raises(RuntimeError, match="closed"):
         s.solve(np.ones(2), np.ones(2), np.zeros(1), np.ones((2, 1)))
+
+
+def test_process_wide_tuning_setters_round_trip():
+    """The lookahead-SM and solve-CTA setters only swap a process-wide value
+    (no device work): each returns the previous value and rejects bad ones."""
+    from aospectrum_b200 import native
+
+    lib = native.library()
+    prev = lib.aosb_factor_set_lookahead_sms(24)
+    assert lib.aosb_factor_set_lookahead_sms(0) == 24
+    assert lib.aosb_factor_set_lookahead_sms(-1) == -1
+    lib.aosb_factor_set_lookahead_sms(prev)
+    prev = lib.aosb_solve_set_ctas_per_sm(1)
+    assert lib.aosb_solve_set_ctas_per_sm(0) == 1
+    assert lib.aosb_solve_set_ctas_per_sm(3) == -1
+    assert lib.aosb_solve_set_ctas_per_sm(prev) == 2   # 0 restored the default, 2
+
+
+@pytest.mark.parametrize("max_rows", [4, 13, 16])
+def test_row_blocks_share_columns_and_respect_the_cap(max_rows):
+    """engine.row_blocks: every block holds consecutive rows with one column
+    set, at most max_rows of them, and the blocks tile 0..n."""
+    from aospectrum_b200.engine import row_blocks
+
+    b = bundles.small2d()
+    pat = bloch_ref.build_pattern(b)
+    indptr, indices = pat.indptr, pat.indices
+    starts = np.asarray(b.basis.atom_offsets)[:-1]
+    for st in (starts, None):
+        rb = row_blocks(indptr, indices, max_rows=max_rows, starts=st)
+        assert rb[0] == 0 and rb[-1] == indptr.size - 1
+        assert np.all(np.diff(rb) >= 1) and np.all(np.diff(rb) <= max_rows)
+        for a, z in zip(rb[:-1], rb[1:]):
+            first = indices[indptr[a]:indptr[a + 1]]
+            for r in range(a + 1, z):
+                assert np.array_equal(indices[indptr[r]:indptr[r + 1]], first)
