@@ -652,9 +652,13 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   // rest of step k's Schur update runs on the others.
   const bool lookahead = tc_panels && sms >= 32;
   const int chosen = g_lookahead_sms.load();
+  // default: 5/4 of the pencils (the side stream's diagonal LU runs one CTA
+  // per pencil), at most a third of the SMs; the reserved SMs join the rest
+  // of the two-step update once the panels are done, so a generous reserve
+  // costs little (c2: 48 SMs beat 37 at 64 pencils, 40 beat 24 and 16 at 32)
   const int reserve = !lookahead ? 0
                       : chosen > 0 ? std::min(chosen, sms / 2)
-                                   : std::min(std::max(np, 8), sms / 4);
+                                   : std::min(std::max(np * 5 / 4, 8), sms / 3);
   cudaStream_t side = nullptr;
   cudaEvent_t ev_cross = nullptr, ev_panel = nullptr;
   if (lookahead) {

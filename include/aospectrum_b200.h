@@ -297,7 +297,7 @@ int aosb_factor(const aosb_plan_t *plan, const aosb_factor_args_v1 *args,
 /* SMs that the tensor-core factorization leaves to its lookahead side
  * stream (next steps' diagonal LU, panel products and staging) while the
  * Schur update runs on the others; 0 restores the default rule
- * min(max(n_pencils, 8), SMs / 4); values are capped at SMs / 2.
+ * min(max(5 n_pencils / 4, 8), SMs / 3); values are capped at SMs / 2.
  * Process-wide; returns the previous setting (-1 for sms < 0).  No
  * counterpart in the reference (cuDSS schedules internally). */
 int32_t aosb_factor_set_lookahead_sms(int32_t sms);
