@@ -152,6 +152,65 @@ __global__ void __launch_bounds__(256, 4) bloch_pairs_kernel(
     const int4 mi = group[gm];
     const int64_t mbase = gdst[gm];
     const int2 mr = gmem[gm];
+    if (rg.y - rg.x == 1 && mr.y - mr.x == 1) {
+      // One member block each way (a single lattice image, the common
+      // case): its value offsets and phases are warp-uniform and loaded
+      // once; each lane keeps two elements' four value loads in flight.
+      const int64_t ox = moff[rg.x], oy = moff[mr.x];
+      const float2* phx = ph0 + msh[rg.x];
+      const float2* phy = ph0 + msh[mr.x];
+      float2 px[kBlochKChunk], py[kBlochKChunk];
+#pragma unroll
+      for (int q = 0; q < kBlochKChunk; ++q) {
+        px[q] = q < nk ? phx[q * n_shifts] : make_float2(0.0f, 0.0f);
+        py[q] = q < nk ? phy[q * n_shifts] : make_float2(0.0f, 0.0f);
+      }
+      for (int t0 = lane; t0 < 4 * ne; t0 += 64) {
+        float2 vx[2], vy[2];
+        float2* out[2];
+        int win[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int t = t0 + 32 * u;
+          out[u] = nullptr;
+          win[u] = 0;
+          vx[u] = vy[u] = make_float2(0.0f, 0.0f);
+          if (t < 4 * ne) {
+            const int which = t >= 2 * ne;
+            const int r = t - which * 2 * ne;
+            win[u] = r >= ne;
+            const int e = r - win[u] * ne;
+            int a, c;
+            int64_t dst;
+            if (win[u] == 0) {
+              a = e / nc;
+              c = e - a * nc;
+              dst = base + (int64_t)a * rl + c;
+            } else {
+              c = e / nr;
+              a = e - c * nr;
+              dst = mbase + (int64_t)c * mi.z + a;
+            }
+            const V* vals = which == 0 ? hv : sv;
+            out[u] = (which == 0 ? hout : sout) + out0 + dst;
+            vx[u] = load_value<V>(vals, ox + a * nc + c);
+            vy[u] = load_value<V>(vals, oy + c * nr + a);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (out[u] == nullptr) continue;
+#pragma unroll
+          for (int q = 0; q < kBlochKChunk; ++q) {
+            if (q < nk) {
+              const float2 mean = hermitian_mean(cmul_rn(vx[u], px[q]), cmul_rn(vy[u], py[q]));
+              out[u][q * nnz] = win[u] == 0 ? mean : make_float2(mean.x, -mean.y);
+            }
+          }
+        }
+      }
+      return;
+    }
     // t runs over [matrix H|S][window (i,j)|(j,i)][row-major element]
     for (int t = lane; t < 4 * ne; t += 32) {
       const int which = t >= 2 * ne;
