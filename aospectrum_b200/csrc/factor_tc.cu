@@ -193,7 +193,12 @@ __global__ void __launch_bounds__(256) stage_kernel(int nL, int nU, int panel, i
 //                  reduce-add on the target tile.
 // Two accumulator sets let the epilogue of one item overlap the MMAs of the
 // next.
-constexpr int kStagesP = 4;
+// Depth of the operand slab ring (build-time: -DAOSB_SCHUR_STAGES=n; 5 is
+// the most that fits beside the epilogue tiles in 227 KB).
+#ifndef AOSB_SCHUR_STAGES
+#define AOSB_SCHUR_STAGES 4
+#endif
+constexpr int kStagesP = AOSB_SCHUR_STAGES;
 constexpr int kEpiWarps = 8;
 constexpr int kPThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemColsP = 512;
