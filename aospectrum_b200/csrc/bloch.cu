@@ -8,11 +8,11 @@
 // CSR arrays, because every row of atom i has the same column structure.
 // Entry (a, c) of group (i, j) sits at dst_base + a * rowlen_i + c.
 //
-// The device kernel gives one warp to each unordered atom pair {i, j} and
-// chunk of up to four k points: it sums the member blocks of (i, j) and of
-// its mirror (j, i) in block order (the order the reference's stable sort
-// leaves them in), applies the Hermitian projection of sparse.py:25-36 and
-// writes both windows row by row for every k point of the chunk.  With
+// The device kernel gives one warp to each group (window) and chunk of up
+// to four k points: it sums the member blocks of (i, j) and of its mirror
+// (j, i) in block order (the order the reference's stable sort leaves them
+// in), applies the Hermitian projection of sparse.py:25-36 and writes the
+// window row by row for every k point of the chunk.  With
 // real block values the products v * phase are exact, so the output is
 // bit-identical to the reference's numpy path.
 #include "common.cuh"
@@ -29,20 +29,18 @@ struct aosb_bloch {
   std::vector<int32_t> shifts;       // n_shifts * 3
   std::vector<int32_t> block_shift;  // n_blocks
   // device tables
-  int64_t n_groups = 0, n_pairs = 0, n_members = 0;
+  int64_t n_groups = 0, n_members = 0;
   int64_t* d_indptr = nullptr;
   int32_t* d_indices = nullptr;
   int4* d_group = nullptr;        // (nr, nc, rowlen, mirror)
   int64_t* d_group_dst = nullptr;  // dst base
   int2* d_group_members = nullptr; // [begin, end) into members
-  int32_t* d_pairs = nullptr;      // group index with i <= j
   int64_t* d_member_off = nullptr; // value offset of each member block
   int32_t* d_member_shift = nullptr;
   // host copies of the device tables (uploaded by aosb_bloch_upload)
   std::vector<int4> g_info;
   std::vector<int64_t> g_dst;
   std::vector<int2> g_mem;
-  std::vector<int32_t> pairs;
   std::vector<int64_t> m_off;
   std::vector<int32_t> m_shift;
   int64_t n_values = 0;  // stored block values (sum of block sizes), set at upload
@@ -122,127 +120,38 @@ __device__ __forceinline__ float2 hermitian_mean(float2 x, float2 y) {
   return make_float2(__fmul_rn(__fadd_rn(x.x, y.x), 0.5f), __fmul_rn(__fsub_rn(x.y, y.y), 0.5f));
 }
 
-// Output element (a, c) of window (i, j) and the conjugate entry (c, a) of
-// window (j, i) need the same Hermitian mean; the kernel recomputes the mean
-// for each window so that every lane writes along window rows (coalesced)
-// instead of transposed.
+// One warp per group (i, j) writes that group's window.  Groups are sorted by
+// (row atom, column atom), so the 8 warps of a CTA write neighbouring windows
+// of the same CSR rows at the same time and the 32-byte sectors they share
+// at window boundaries are completed in L2 instead of leaving it partly
+// written.  Element (a, c) of window (i, j) and element (c, a) of its mirror
+// (j, i) hold the Hermitian mean of the pair and its conjugate: the upper
+// window (i < j) writes mean(x_ij(a, c), x_ji(c, a)), the lower window writes
+// the conjugate of its upper mirror's mean formed the same way.
 template <typename V>
-__global__ void __launch_bounds__(256, 4) bloch_pairs_kernel(
-    int64_t n_pairs, const int32_t* __restrict__ pairs, const int4* __restrict__ group,
-    const int64_t* __restrict__ gdst, const int2* __restrict__ gmem,
-    const int64_t* __restrict__ moff, const int32_t* __restrict__ msh,
-    const V* __restrict__ hv, const V* __restrict__ sv, const float2* __restrict__ phases,
-    int64_t n_shifts, int64_t nnz, int n_k, float2* __restrict__ hout,
-    float2* __restrict__ sout) {
+__global__ void __launch_bounds__(256, 4) bloch_windows_kernel(
+    int64_t n_groups, const int4* __restrict__ group, const int64_t* __restrict__ gdst,
+    const int2* __restrict__ gmem, const int64_t* __restrict__ moff,
+    const int32_t* __restrict__ msh, const V* __restrict__ hv, const V* __restrict__ sv,
+    const float2* __restrict__ phases, int64_t n_shifts, int64_t nnz, int n_k,
+    float2* __restrict__ hout, float2* __restrict__ sout) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (warp >= n_pairs) return;
+  if (warp >= n_groups) return;
   const int k0 = blockIdx.y * kBlochKChunk;
   const int nk = min(n_k - k0, kBlochKChunk);
   const float2* ph0 = phases + (int64_t)k0 * n_shifts;
   const int64_t out0 = (int64_t)k0 * nnz;
-  const int g = pairs[warp];
+  const int g = (int)warp;
   const int4 gi = group[g];  // nr, nc, rowlen, mirror
   const int nr = gi.x, nc = gi.y, rl = gi.z, gm = gi.w;
   const int ne = nr * nc;
   const int64_t base = gdst[g];
   const int2 rg = gmem[g];
   float2 x[kBlochKChunk], y[kBlochKChunk];
-  if (gm != g) {
-    const int4 mi = group[gm];
-    const int64_t mbase = gdst[gm];
-    const int2 mr = gmem[gm];
-    if (rg.y - rg.x == 1 && mr.y - mr.x == 1) {
-      // One member block each way (a single lattice image, the common
-      // case): its value offsets and phases are warp-uniform and loaded
-      // once; each lane keeps two elements' four value loads in flight.
-      const int64_t ox = moff[rg.x], oy = moff[mr.x];
-      const float2* phx = ph0 + msh[rg.x];
-      const float2* phy = ph0 + msh[mr.x];
-      float2 px[kBlochKChunk], py[kBlochKChunk];
-#pragma unroll
-      for (int q = 0; q < kBlochKChunk; ++q) {
-        px[q] = q < nk ? phx[q * n_shifts] : make_float2(0.0f, 0.0f);
-        py[q] = q < nk ? phy[q * n_shifts] : make_float2(0.0f, 0.0f);
-      }
-      for (int t0 = lane; t0 < 4 * ne; t0 += 64) {
-        float2 vx[2], vy[2];
-        float2* out[2];
-        int win[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int t = t0 + 32 * u;
-          out[u] = nullptr;
-          win[u] = 0;
-          vx[u] = vy[u] = make_float2(0.0f, 0.0f);
-          if (t < 4 * ne) {
-            const int which = t >= 2 * ne;
-            const int r = t - which * 2 * ne;
-            win[u] = r >= ne;
-            const int e = r - win[u] * ne;
-            int a, c;
-            int64_t dst;
-            if (win[u] == 0) {
-              a = e / nc;
-              c = e - a * nc;
-              dst = base + (int64_t)a * rl + c;
-            } else {
-              c = e / nr;
-              a = e - c * nr;
-              dst = mbase + (int64_t)c * mi.z + a;
-            }
-            const V* vals = which == 0 ? hv : sv;
-            out[u] = (which == 0 ? hout : sout) + out0 + dst;
-            vx[u] = load_value<V>(vals, ox + a * nc + c);
-            vy[u] = load_value<V>(vals, oy + c * nr + a);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          if (out[u] == nullptr) continue;
-#pragma unroll
-          for (int q = 0; q < kBlochKChunk; ++q) {
-            if (q < nk) {
-              const float2 mean = hermitian_mean(cmul_rn(vx[u], px[q]), cmul_rn(vy[u], py[q]));
-              out[u][q * nnz] = win[u] == 0 ? mean : make_float2(mean.x, -mean.y);
-            }
-          }
-        }
-      }
-      return;
-    }
-    // t runs over [matrix H|S][window (i,j)|(j,i)][row-major element]
-    for (int t = lane; t < 4 * ne; t += 32) {
-      const int which = t >= 2 * ne;
-      const int r = t - which * 2 * ne;
-      const int win = r >= ne;
-      const int e = r - win * ne;
-      int a, c;
-      int64_t dst;
-      if (win == 0) {
-        a = e / nc;
-        c = e - a * nc;
-        dst = base + (int64_t)a * rl + c;
-      } else {
-        c = e / nr;
-        a = e - c * nr;
-        dst = mbase + (int64_t)c * mi.z + a;
-      }
-      const V* vals = which == 0 ? hv : sv;
-      float2* out = (which == 0 ? hout : sout) + out0 + dst;
-      group_sums<V>(vals, moff, msh, ph0, n_shifts, nk, rg, a * nc + c, x);
-      group_sums<V>(vals, moff, msh, ph0, n_shifts, nk, mr, c * nr + a, y);
-#pragma unroll
-      for (int q = 0; q < kBlochKChunk; ++q) {
-        if (q < nk) {
-          const float2 mean = hermitian_mean(x[q], y[q]);
-          out[q * nnz] = win == 0 ? mean : make_float2(mean.x, -mean.y);
-        }
-      }
-    }
-  } else {
-    // t runs over [matrix H|S][row-major element]; the mean of the pair
-    // (lo, hi) is formed the same way for both of its entries
+  if (gm == g) {
+    // diagonal window: t runs over [matrix H|S][row-major element]; the mean
+    // of the pair (lo, hi) is formed the same way for both of its entries
     for (int t = lane; t < 2 * ne; t += 32) {
       const int which = t >= ne;
       const int e = t - which * ne;
@@ -264,6 +173,75 @@ __global__ void __launch_bounds__(256, 4) bloch_pairs_kernel(
           }
           out[q * nnz] = v;
         }
+      }
+    }
+    return;
+  }
+  const bool lower = gm < g;
+  const int2 mr = gmem[gm];
+  // the mean's first operand comes from the upper group of the pair
+  const int2 r1 = lower ? mr : rg, r2 = lower ? rg : mr;
+  if (r1.y - r1.x == 1 && r2.y - r2.x == 1) {
+    // One member block each way (a single lattice image, the common case):
+    // value offsets and phases are warp-uniform and loaded once; each lane
+    // keeps two elements' value loads in flight.
+    const int64_t o1 = moff[r1.x], o2 = moff[r2.x];
+    const float2* ph1 = ph0 + msh[r1.x];
+    const float2* ph2 = ph0 + msh[r2.x];
+    float2 p1[kBlochKChunk], p2[kBlochKChunk];
+#pragma unroll
+    for (int q = 0; q < kBlochKChunk; ++q) {
+      p1[q] = q < nk ? ph1[q * n_shifts] : make_float2(0.0f, 0.0f);
+      p2[q] = q < nk ? ph2[q * n_shifts] : make_float2(0.0f, 0.0f);
+    }
+    for (int t0 = lane; t0 < 2 * ne; t0 += 64) {
+      float2 v1[2], v2[2];
+      float2* out[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int t = t0 + 32 * u;
+        out[u] = nullptr;
+        v1[u] = v2[u] = make_float2(0.0f, 0.0f);
+        if (t < 2 * ne) {
+          const int which = t >= ne;
+          const int e = t - which * ne;
+          const int a = e / nc, c = e - a * nc;
+          const int eg = a * nc + c, em = c * nr + a;
+          const V* vals = which == 0 ? hv : sv;
+          out[u] = (which == 0 ? hout : sout) + out0 + base + (int64_t)a * rl + c;
+          v1[u] = load_value<V>(vals, o1 + (lower ? em : eg));
+          v2[u] = load_value<V>(vals, o2 + (lower ? eg : em));
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        if (out[u] == nullptr) continue;
+#pragma unroll
+        for (int q = 0; q < kBlochKChunk; ++q) {
+          if (q < nk) {
+            const float2 mean = hermitian_mean(cmul_rn(v1[u], p1[q]), cmul_rn(v2[u], p2[q]));
+            out[u][q * nnz] = lower ? make_float2(mean.x, -mean.y) : mean;
+          }
+        }
+      }
+    }
+    return;
+  }
+  // general: t runs over [matrix H|S][row-major element]
+  for (int t = lane; t < 2 * ne; t += 32) {
+    const int which = t >= ne;
+    const int e = t - which * ne;
+    const int a = e / nc, c = e - a * nc;
+    const int eg = a * nc + c, em = c * nr + a;
+    const V* vals = which == 0 ? hv : sv;
+    float2* out = (which == 0 ? hout : sout) + out0 + base + (int64_t)a * rl + c;
+    group_sums<V>(vals, moff, msh, ph0, n_shifts, nk, r1, lower ? em : eg, x);
+    group_sums<V>(vals, moff, msh, ph0, n_shifts, nk, r2, lower ? eg : em, y);
+#pragma unroll
+    for (int q = 0; q < kBlochKChunk; ++q) {
+      if (q < nk) {
+        const float2 mean = hermitian_mean(x[q], y[q]);
+        out[q * nnz] = lower ? make_float2(mean.x, -mean.y) : mean;
       }
     }
   }
@@ -378,7 +356,6 @@ int aosb_bloch_create(int64_t n_orbitals, int64_t n_atoms, const int64_t* atom_o
   // Mirror groups (Hermitian topology).
   std::vector<int4> g_info(ng);
   std::vector<int64_t> g_dst(ng);
-  std::vector<int32_t> pairs;
   for (int64_t g = 0; g < ng; ++g) {
     const int32_t i = g_row[g], j = g_col[g];
     int64_t lo = first_group[j], hi = first_group[j + 1];
@@ -396,14 +373,11 @@ int aosb_bloch_create(int64_t n_orbitals, int64_t n_atoms, const int64_t* atom_o
     const int nc = (int)(atom_offsets[j + 1] - atom_offsets[j]);
     g_info[g] = make_int4(nr, nc, (int)rowlen[i], (int)m);
     g_dst[g] = B->indptr[atom_offsets[i]] + colpos[g];
-    if (i <= j) pairs.push_back((int32_t)g);
   }
-  B->n_pairs = (int64_t)pairs.size();
   B->n_members = (int64_t)m_off.size();
   B->g_info = std::move(g_info);
   B->g_dst = std::move(g_dst);
   B->g_mem = std::move(g_mem);
-  B->pairs = std::move(pairs);
   B->m_off = std::move(m_off);
   B->m_shift = std::move(m_shift);
   *out = B;
@@ -419,7 +393,6 @@ int aosb_bloch_upload(aosb_bloch_t* B, char* err, size_t cap) {
       (rc = upload(&B->d_group, B->g_info, err, cap)) ||
       (rc = upload(&B->d_group_dst, B->g_dst, err, cap)) ||
       (rc = upload(&B->d_group_members, B->g_mem, err, cap)) ||
-      (rc = upload(&B->d_pairs, B->pairs, err, cap)) ||
       (rc = upload(&B->d_member_off, B->m_off, err, cap)) ||
       (rc = upload(&B->d_member_shift, B->m_shift, err, cap)))
     return rc;
@@ -469,19 +442,19 @@ int aosb_bloch_apply(const aosb_bloch_t* b, int32_t value_kind, const void* h_va
   if (n_k <= 0 || n_k > 65535)
     return aosb::set_error(err, cap, AOSB_ERR_ARGUMENT, "n_k must be in 1..65535");
   const int warps = 8;
-  dim3 grid(aosb::ceil_div(b->n_pairs, warps), aosb::ceil_div(n_k, kBlochKChunk));
+  dim3 grid(aosb::ceil_div(b->n_groups, warps), aosb::ceil_div(n_k, kBlochKChunk));
   cudaStream_t st = (cudaStream_t)stream;
   const int64_t nsh = (int64_t)(b->shifts.size() / 3);
   cudaEvent_t ev[2];
   const bool timed = aosb::timing_begin(st, ev);
   if (value_kind == 0) {
-    bloch_pairs_kernel<float><<<grid, warps * 32, 0, st>>>(
-        b->n_pairs, b->d_pairs, b->d_group, b->d_group_dst, b->d_group_members, b->d_member_off,
+    bloch_windows_kernel<float><<<grid, warps * 32, 0, st>>>(
+        b->n_groups, b->d_group, b->d_group_dst, b->d_group_members, b->d_member_off,
         b->d_member_shift, (const float*)h_values, (const float*)s_values,
         (const float2*)phases, nsh, b->nnz, n_k, (float2*)h_out, (float2*)s_out);
   } else if (value_kind == 1) {
-    bloch_pairs_kernel<float2><<<grid, warps * 32, 0, st>>>(
-        b->n_pairs, b->d_pairs, b->d_group, b->d_group_dst, b->d_group_members, b->d_member_off,
+    bloch_windows_kernel<float2><<<grid, warps * 32, 0, st>>>(
+        b->n_groups, b->d_group, b->d_group_dst, b->d_group_members, b->d_member_off,
         b->d_member_shift, (const float2*)h_values, (const float2*)s_values,
         (const float2*)phases, nsh, b->nnz, n_k, (float2*)h_out, (float2*)s_out);
   } else {
@@ -494,7 +467,7 @@ int aosb_bloch_apply(const aosb_bloch_t* b, int32_t value_kind, const void* h_va
     aosb::timing_end(aosb::kTimedBloch, st, ev, 0.0,
                      (double)b->n_values * 2.0 * (value_kind ? 8.0 : 4.0) +
                          (double)n_k * (double)b->nnz * 2.0 * 8.0);
-  return aosb::launch_check(err, cap, "bloch_pairs_kernel");
+  return aosb::launch_check(err, cap, "bloch_windows_kernel");
 }
 
 void aosb_bloch_destroy(aosb_bloch_t* b) {
@@ -504,7 +477,6 @@ void aosb_bloch_destroy(aosb_bloch_t* b) {
   cudaFree(b->d_group);
   cudaFree(b->d_group_dst);
   cudaFree(b->d_group_members);
-  cudaFree(b->d_pairs);
   cudaFree(b->d_member_off);
   cudaFree(b->d_member_shift);
   delete b;

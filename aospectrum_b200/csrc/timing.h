@@ -13,7 +13,7 @@ enum TimedKernel : int {
   kTimedSolveUpdate = 2,  // solve_update_kernel / solve_tc_kernel
   kTimedResidual = 3,     // shifted_residual(_blocks)_kernel
   kTimedSpmm = 4,         // spmm_kernel
-  kTimedBloch = 5,        // bloch_pairs_kernel
+  kTimedBloch = 5,        // bloch_windows_kernel
   kTimedCount = 6,
 };
 
