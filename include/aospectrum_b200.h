@@ -290,6 +290,11 @@ typedef struct {
 } aosb_factor_args_v1;
 
 size_t aosb_factor_bytes(const aosb_plan_t *plan, int32_t n_pencils);
+/* Tensor-core precisions: four staging buffers of split-BF16 panel tiles
+ * plus 256 bytes for the item counter that the two-step update's main and
+ * lookahead launches share; 0 for precision 0.  A workspace sized for
+ * n_pencils serves any batch of at most n_pencils; one factorization at a
+ * time per workspace. */
 size_t aosb_factor_workspace_bytes(const aosb_plan_t *plan, int32_t n_pencils,
                                    int32_t precision);
 int aosb_factor(const aosb_plan_t *plan, const aosb_factor_args_v1 *args,
