@@ -13,6 +13,7 @@ solved in FP64 on the host from FP64 device products.
 
 from __future__ import annotations
 
+import contextlib
 import math
 from dataclasses import dataclass, field
 from typing import Any
@@ -186,11 +187,14 @@ def small_lapack():
     return threadpool_limits(limits=1)
 
 
-def truncate_gram(gram: np.ndarray, tolerance: float) -> tuple[np.ndarray, np.ndarray]:
+def truncate_gram(gram: np.ndarray, tolerance: float, *,
+                  limit_threads: bool = True) -> tuple[np.ndarray, np.ndarray]:
     """Rank truncation of the S-Gram matrix of the moments (reference
     ``_compress_moments``, ciss.py:107-126): returns the transform
-    V_keep / sqrt(lambda) and the singular values sqrt(lambda)."""
-    with small_lapack():
+    V_keep / sqrt(lambda) and the singular values sqrt(lambda).
+    ``limit_threads=False`` leaves the BLAS thread limit to the caller (a
+    caller running several of these in threads sets it once around them)."""
+    with small_lapack() if limit_threads else contextlib.nullcontext():
         values, vectors = np.linalg.eigh(hermitize(gram))
     scale = float(np.max(np.abs(values), initial=0.0))
     if scale == 0.0 or not math.isfinite(scale):
@@ -202,13 +206,14 @@ def truncate_gram(gram: np.ndarray, tolerance: float) -> tuple[np.ndarray, np.nd
     return vectors[:, keep] / np.sqrt(lam)[None, :], np.sqrt(lam)
 
 
-def projected_eigh(hr: np.ndarray, sr: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+def projected_eigh(hr: np.ndarray, sr: np.ndarray, *,
+                   limit_threads: bool = True) -> tuple[np.ndarray, np.ndarray]:
     """Generalized Hermitian eigenproblem of the projected pencil (reference
     ``_rayleigh_ritz``, ciss.py:129-150), solved in FP64."""
     from scipy import linalg
 
     try:
-        with small_lapack():
+        with small_lapack() if limit_threads else contextlib.nullcontext():
             e, c = linalg.eigh(hermitize(hr), hermitize(sr), check_finite=False, driver="gvd")
     except linalg.LinAlgError as exc:
         raise SolverError("CISS reduced overlap is not positive definite") from exc

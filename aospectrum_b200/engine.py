@@ -23,6 +23,8 @@ of the reference (``src/aospectrum/sparse.py:199-245``,
 from __future__ import annotations
 
 import math
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 from time import perf_counter
 from typing import Any, Sequence
@@ -40,6 +42,7 @@ from .ciss import (
     probe_block,
     projected_eigh,
     result_warnings,
+    small_lapack,
     truncate_gram,
 )
 from .data import EnergyInterval, LocalizedOperatorBundle
@@ -424,6 +427,7 @@ class BandEngine:
         self.probes = torch.from_numpy(q.astype(np.complex128)).to(self.device)
         self._gram_scratch = None
         self._solve_scratch = None
+        self._lapack_pool: ThreadPoolExecutor | None = None
         self.last_stats: dict[str, Any] = {}
         # optional device timing of every factorization call (CUDA events)
         self.profile_factor = False
@@ -652,9 +656,7 @@ class BandEngine:
                                     + stages.get("native_multi_rhs_solve", 0.0)
                                     + stages.get("moment_accumulation", 0.0))
         del factor, pivots, wn, xn, rr, workspace
-        results = []
-        for k in range(nk):
-            results.append(self._subspace(hvals[k], svals[k], mom[k], interval, stages, nk))
+        results = self._subspace_batch(hvals, svals, mom, interval, stages, nk)
         peak = int(torch.cuda.max_memory_allocated(dev))
         total = perf_counter() - total0
         for res in results:
@@ -714,54 +716,100 @@ class BandEngine:
                         self.pattern.nnz, pk.data_ptr(), z.contiguous().data_ptr(),
                         b.data_ptr(), n * L, xn.data_ptr(), rr.data_ptr(), st)
 
-    def _subspace(self, h, s, mom, interval: EnergyInterval, stages: dict[str, float],
-                  nk: int) -> CissResult:
-        """Rank truncation, Rayleigh-Ritz, ghost filter and residuals for one k."""
+    def _host_map(self, fn, items: list) -> list:
+        """fn over items: the small FP64 eigenproblems of the batch's k points
+        run in parallel threads, each on one BLAS thread (numpy and scipy
+        release the GIL inside LAPACK)."""
+        if len(items) <= 1:
+            return [fn(x) for x in items]
+        if self._lapack_pool is None:
+            self._lapack_pool = ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1))
+        with small_lapack():
+            return list(self._lapack_pool.map(fn, items))
+
+    def _subspace_batch(self, hvals, svals, mom, interval: EnergyInterval,
+                        stages: dict[str, float], nk: int) -> list[CissResult]:
+        """Rank truncation, Rayleigh-Ritz, ghost filter and residuals for the
+        batch's k points, in lockstep: each phase enqueues the device work of
+        every k point, reads the small results back once and solves the k
+        points' host eigenproblems in parallel.  Per k point the arithmetic
+        is that of the reference's solve_interval (ciss.py:320-372)."""
         torch = _torch()
         st = self.settings
         dev = self.device
-        local: dict[str, float] = {k: v / nk for k, v in stages.items()}
+        local = [{k: v / nk for k, v in stages.items()} for _ in range(nk)]
+        # compression: G = M^H S M, truncation, B = M V / sqrt(lambda)
         t = perf_counter()
-        sm = torch.empty_like(mom)
-        self._spmm(s, mom, sm)
-        gram = self._gram(mom, sm).cpu().numpy()
-        transform, sigma = truncate_gram(gram, st.rank_relative_tolerance)
-        basis = self._dense_mul(mom, torch.from_numpy(transform).to(dev))
-        saturated = basis.shape[1] == st.search_dimension
+        grams = []
+        for k in range(nk):
+            sm = torch.empty_like(mom[k])
+            self._spmm(svals[k], mom[k], sm)
+            grams.append(self._gram(mom[k], sm))
+        grams = torch.stack(grams).cpu().numpy()
+        tol = st.rank_relative_tolerance
+        trunc = self._host_map(lambda g: truncate_gram(g, tol, limit_threads=False), list(grams))
+        basis = [self._dense_mul(mom[k], torch.from_numpy(trunc[k][0]).to(dev)) for k in range(nk)]
         torch.cuda.current_stream(dev).synchronize()
-        local["subspace_compression"] = perf_counter() - t
+        dt = (perf_counter() - t) / nk
+        for d in local:
+            d["subspace_compression"] = dt
+        # Rayleigh-Ritz: B^H H B, B^H S B, generalized eigh in FP64
         t = perf_counter()
-        hb = torch.empty_like(basis)
-        sb = torch.empty_like(basis)
-        self._spmm(h, basis, hb)
-        self._spmm(s, basis, sb)
-        hr = self._gram(basis, hb).cpu().numpy()
-        sr = self._gram(basis, sb).cpu().numpy()
-        energies, coeffs = projected_eigh(hr, sr)
-        local["rayleigh_ritz"] = perf_counter() - t
-        keep = nonspurious_mask(coeffs, sigma, st.spurious_relative_threshold)
-        inside = (energies > interval.lower_ev) & (energies < interval.upper_ev)
-        sel = np.flatnonzero(keep & inside)
-        max_res = 0.0
-        if sel.size:
-            t = perf_counter()
-            csel = torch.from_numpy(np.ascontiguousarray(coeffs[:, sel])).to(dev)
-            vec = self._dense_mul(basis, csel)
+        pairs = []
+        for k in range(nk):
+            hb = torch.empty_like(basis[k])
+            sb = torch.empty_like(basis[k])
+            self._spmm(hvals[k], basis[k], hb)
+            self._spmm(svals[k], basis[k], sb)
+            pairs.append((self._gram(basis[k], hb), self._gram(basis[k], sb)))
+        pairs = [(hr.cpu().numpy(), sr.cpu().numpy()) for hr, sr in pairs]
+        eig = self._host_map(lambda p: projected_eigh(p[0], p[1], limit_threads=False), pairs)
+        dt = (perf_counter() - t) / nk
+        for d in local:
+            d["rayleigh_ritz"] = dt
+        # ghost filter, interval selection, FP64 eigenpair residuals
+        sel = []
+        for k in range(nk):
+            energies, coeffs = eig[k]
+            keep = nonspurious_mask(coeffs, trunc[k][1], st.spurious_relative_threshold)
+            inside = (energies > interval.lower_ev) & (energies < interval.upper_ev)
+            sel.append(np.flatnonzero(keep & inside))
+        t = perf_counter()
+        norms = [None] * nk
+        for k in range(nk):
+            if not sel[k].size:
+                continue
+            energies, coeffs = eig[k]
+            csel = torch.from_numpy(np.ascontiguousarray(coeffs[:, sel[k]])).to(dev)
+            vec = self._dense_mul(basis[k], csel)
             hv = torch.empty_like(vec)
             sv = torch.empty_like(vec)
-            self._spmm(h, vec, hv)
-            self._spmm(s, vec, sv)
-            e_d = torch.from_numpy(np.ascontiguousarray(energies[sel])).to(dev)
-            norms = torch.empty(sel.size, dtype=torch.float64, device=dev)
-            native.call("aosb_column_norms", self.n, int(sel.size), hv.data_ptr(), sv.data_ptr(),
-                        hv.stride(0), e_d.data_ptr(), norms.data_ptr(), self._stream())
-            max_res = float(norms.max().item())
-            local["residual"] = perf_counter() - t
-        selected = np.asarray(energies[sel], dtype=np.float32)
-        return CissResult(selected, max_res, local, None, result_warnings(max_res, saturated),
-                          not saturated)
+            self._spmm(hvals[k], vec, hv)
+            self._spmm(svals[k], vec, sv)
+            e_d = torch.from_numpy(np.ascontiguousarray(energies[sel[k]])).to(dev)
+            norms[k] = torch.empty(sel[k].size, dtype=torch.float64, device=dev)
+            native.call("aosb_column_norms", self.n, int(sel[k].size), hv.data_ptr(),
+                        sv.data_ptr(), hv.stride(0), e_d.data_ptr(), norms[k].data_ptr(),
+                        self._stream())
+        max_res = [float(x.max().item()) if x is not None else 0.0 for x in norms]
+        n_res = sum(1 for x in norms if x is not None)
+        if n_res:
+            dt = (perf_counter() - t) / n_res
+            for k in range(nk):
+                if norms[k] is not None:
+                    local[k]["residual"] = dt
+        results = []
+        for k in range(nk):
+            saturated = basis[k].shape[1] == st.search_dimension
+            selected = np.asarray(eig[k][0][sel[k]], dtype=np.float32)
+            results.append(CissResult(selected, max_res[k], local[k], None,
+                                      result_warnings(max_res[k], saturated), not saturated))
+        return results
 
     def close(self) -> None:
+        if self._lapack_pool is not None:
+            self._lapack_pool.shutdown(wait=True)
+            self._lapack_pool = None
         if self._owns:
             self.pattern.close()
             self.plan.close()
