@@ -19,10 +19,12 @@
 //                   width rounded up to 16) per slab into one of two TMEM
 //                   accumulator pairs (re, im): hi*hi + hi*lo + lo*hi per real
 //                   product, FP32 accumulation;
-//   warps 6-9       epilogue: tcgen05.ld of the accumulator (warp w reads
-//                   lanes 32 (w % 4) ..); -acc goes through 128B-swizzled
-//                   shared boxes into TMA reduce-adds on X_i (coalesced and
-//                   asynchronous: X never passes through the registers).
+//   warps 6-9       epilogue: first the CTA's slice of the copy X_k = Y
+//                   (the step's diagonal result), then per item tcgen05.ld
+//                   of the accumulator (warp w reads lanes 32 (w % 4) ..);
+//                   -acc goes through 128B-swizzled shared boxes into TMA
+//                   reduce-adds on X_i (coalesced and asynchronous: X never
+//                   passes through the registers).
 // Two accumulator pairs let one item's epilogue overlap the next item's
 // MMAs.  Every mbarrier wait is bounded: on expiry the CTA records
 // AOSB_ERR_TIMEOUT in the pencil status and stops; a CTA that stops waits
@@ -51,7 +53,6 @@ constexpr int kAPlane = kT * kSK * 2;      // 4096 bytes: one BF16 plane of one 
 constexpr int kASlab = 4 * kAPlane;        // 16 KB
 constexpr int kRawPlane = kT * kSK;        // floats in one FP32 plane box of a slab
 constexpr uint32_t kRawBytes = 2 * kRawPlane * sizeof(float);  // 16 KB per slab
-constexpr int kCopyCtas = 4;
 
 enum SolveOp { kOpPlain = 0, kOpConjT = 1 };
 
@@ -131,18 +132,7 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
     const __grid_constant__ CUtensorMap xmap, int x_tma) {
   const int strips = (nrhs + kNS - 1) / kNS;
   const int total = n_items * strips * n_pencils;
-  const int work_ctas = (int)gridDim.x - kCopyCtas;
-  if ((int)blockIdx.x >= work_ctas) {
-    // copy-back CTAs: X_k = Y for every pencil
-    const int cb = blockIdx.x - work_ctas;
-    const int per = kT * nrhs;
-    for (int64_t e = (int64_t)cb * blockDim.x + threadIdx.x; e < (int64_t)per * n_pencils;
-         e += (int64_t)kCopyCtas * blockDim.x) {
-      const int p = (int)(e / per), r = (int)(e % per);
-      work[((size_t)p * n_pad + (size_t)k * kT) * nrhs + r] = ytmp[(size_t)p * per + r];
-    }
-    return;
-  }
+  const int work_ctas = (int)gridDim.x;
   using C = SolveCfg<CTAS>;
   constexpr int kRawStages = C::kRawStages, kAStages = C::kAStages, kBStages = C::kBStages;
   extern __shared__ unsigned char dyn[];
@@ -328,6 +318,31 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
     const int row = quarter * 32 + lane;
     const int sw = lane & 7;
+    {
+      // While the first accumulator fills, the epilogue warps of every CTA
+      // copy one slice of the step's diagonal result into X_k (X_k = Y for
+      // every pencil; no item of this step touches rows of tile k): the
+      // copy rides along with the launch instead of adding CTAs that would
+      // wait for the persistent ones to leave.
+      const int et = threadIdx.x - kEpiWarp0 * 32;  // 0 .. 127
+      const int64_t per = (int64_t)kT * nrhs;      // float2 per pencil
+      if ((nrhs & 1) == 0) {
+        const int64_t per4 = per / 2, n4 = per4 * n_pencils;
+        const int64_t e0 = n4 * blockIdx.x / work_ctas, e1 = n4 * (blockIdx.x + 1) / work_ctas;
+        for (int64_t e = e0 + et; e < e1; e += kEpiWarps * 32) {
+          const int64_t p = e / per4, r = e - p * per4;
+          reinterpret_cast<float4*>(work + ((size_t)p * n_pad + (size_t)k * kT) * nrhs)[r] =
+              reinterpret_cast<const float4*>(ytmp + (size_t)p * per)[r];
+        }
+      } else {
+        const int64_t n2 = per * n_pencils;
+        const int64_t e0 = n2 * blockIdx.x / work_ctas, e1 = n2 * (blockIdx.x + 1) / work_ctas;
+        for (int64_t e = e0 + et; e < e1; e += kEpiWarps * 32) {
+          const int64_t p = e / per, r = e - p * per;
+          work[((size_t)p * n_pad + (size_t)k * kT) * nrhs + r] = ytmp[(size_t)p * per + r];
+        }
+      }
+    }
     int j = 0;
     for (int it = blockIdx.x; it < total; it += work_ctas, ++j) {
       const ItemOf w = item_of(it, n_items, strips);
@@ -456,8 +471,9 @@ int solve_tc_launch(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
   const int strips = (nrhs + kNS - 1) / kNS;
   const int64_t items = (int64_t)n * strips * np;
   const int64_t slots = (int64_t)CTAS * sms;
-  const int work_ctas = (int)(items < slots ? items : slots);
-  dim3 g((unsigned)(work_ctas + kCopyCtas));
+  // at least one CTA: a step without tiles still copies Y into X_k
+  const int work_ctas = (int)(items < slots ? (items > 0 ? items : 1) : slots);
+  dim3 g((unsigned)work_ctas);
   solve_tc_kernel<OP, CTAS><<<g, kSThreads, smem, st>>>(k, n, nrhs, np, P->n_pad, dtiles, dslots,
                                                         P->n_slots, work, ytmp, ystaged, status,
                                                         fmap, xmap, x_tma);
