@@ -150,3 +150,34 @@ def test_band_output_format_matches_reference(tmp_path, golden):
     assert set(summary) == set(ref_summary)
     assert summary["backend"] == "ciss-b200" and summary["scalar_dtype"] == "complex64"
     assert summary_dict(res)["kpoint_count"] == kp.n_points
+
+
+def test_parallel_small_eigensolves_match_serial():
+    """BandEngine._host_map runs the k points' small FP64 eigenproblems in
+    threads under one BLAS thread limit: same results, in order, as the
+    serial calls with their own limit; errors propagate."""
+    from aospectrum_b200.ciss import projected_eigh, truncate_gram
+    from aospectrum_b200.engine import BandEngine
+    from aospectrum_b200.errors import SolverError
+
+    eng = BandEngine.__new__(BandEngine)   # host part only: no device state
+    eng._lapack_pool = None
+    rng = np.random.default_rng(12)
+    grams, pencils = [], []
+    for _ in range(5):
+        m = rng.standard_normal((40, 24)) + 1j * rng.standard_normal((40, 24))
+        grams.append(m.conj().T @ m)
+        h = rng.standard_normal((24, 24)) + 1j * rng.standard_normal((24, 24))
+        pencils.append((h + h.conj().T, grams[-1] + 24 * np.eye(24)))
+    par = eng._host_map(lambda g: truncate_gram(g, 1e-5, limit_threads=False), grams)
+    for g, (t, s) in zip(grams, par):
+        t0, s0 = truncate_gram(g, 1e-5)
+        assert np.array_equal(t, t0) and np.array_equal(s, s0)
+    par = eng._host_map(lambda p: projected_eigh(p[0], p[1], limit_threads=False), pencils)
+    for p, (e, c) in zip(pencils, par):
+        e0, c0 = projected_eigh(*p)
+        assert np.array_equal(e, e0) and np.array_equal(c, c0)
+    with pytest.raises(SolverError):
+        eng._host_map(lambda g: truncate_gram(g, 1e-5, limit_threads=False),
+                      [grams[0], np.zeros((24, 24), complex)])
+    eng._lapack_pool.shutdown()
