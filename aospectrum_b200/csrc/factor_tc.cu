@@ -629,17 +629,19 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   const int np = a->n_pencils;
   const size_t smem = sizeof(PShared) + 1024;
   static_assert(sizeof(PShared) + 1024 <= 232448, "shared memory budget");
-  static bool attr_done = false;
-  if (!attr_done) {
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  // kernel attributes belong to each device's context: set once per device
+  static std::atomic<uint64_t> attr_devices{0};
+  const uint64_t dev_bit = device < 64 ? (uint64_t)1 << device : 0;
+  if (dev_bit == 0 || (attr_devices.load() & dev_bit) == 0) {
     cudaError_t e = cudaFuncSetAttribute(schur_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess)
       return set_error(err, cap, AOSB_ERR_CUDA, "schur_tc smem attribute: %s", cudaGetErrorString(e));
-    attr_done = true;
+    attr_devices.fetch_or(dev_bit);
   }
-  int device = 0, sms = 148;
-  cudaGetDevice(&device);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   // staged tiles per pencil: the step's L and U tiles plus the two
   // diagonal inverses of the panel product
   const int64_t pencil_stride = staged_tiles_per_pencil(P) * (int64_t)kStagedTileBytes;

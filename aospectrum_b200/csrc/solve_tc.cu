@@ -456,9 +456,13 @@ int solve_tc_launch(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
                     const unsigned char* ystaged, int32_t* status, const CUtensorMap& fmap,
                     const CUtensorMap& xmap, int x_tma, int sms, cudaStream_t st, char* err,
                     size_t cap) {
-  static bool attr_done = false;
   const size_t smem = solve_tc_smem<CTAS>();
-  if (!attr_done) {
+  // kernel attributes belong to each device's context: set once per device
+  static std::atomic<uint64_t> attr_devices{0};
+  int device = 0;
+  cudaGetDevice(&device);
+  const uint64_t dev_bit = device < 64 ? (uint64_t)1 << device : 0;
+  if (dev_bit == 0 || (attr_devices.load() & dev_bit) == 0) {
     cudaError_t e = cudaFuncSetAttribute(solve_tc_kernel<OP, CTAS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess && CTAS > 1)
@@ -466,7 +470,7 @@ int solve_tc_launch(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
                                cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess)
       return set_error(err, cap, AOSB_ERR_CUDA, "solve_tc attributes: %s", cudaGetErrorString(e));
-    attr_done = true;
+    attr_devices.fetch_or(dev_bit);
   }
   const int strips = (nrhs + kNS - 1) / kNS;
   const int64_t items = (int64_t)n * strips * np;
