@@ -421,6 +421,30 @@ int aosb_bloch_export(const aosb_bloch_t* b, int64_t* indptr, int32_t* indices, 
   return 0;
 }
 
+int aosb_bloch_export_groups(const aosb_bloch_t* b, int64_t* n_groups, int64_t* n_members,
+                             int32_t* group_info, int64_t* group_dst, int32_t* group_members,
+                             int64_t* member_off, int32_t* member_shift) {
+  if (b == nullptr) return AOSB_ERR_NULL;
+  if (n_groups) *n_groups = (int64_t)b->g_info.size();
+  if (n_members) *n_members = (int64_t)b->m_off.size();
+  for (size_t g = 0; g < b->g_info.size(); ++g) {
+    if (group_info) {
+      group_info[4 * g] = b->g_info[g].x;
+      group_info[4 * g + 1] = b->g_info[g].y;
+      group_info[4 * g + 2] = b->g_info[g].z;
+      group_info[4 * g + 3] = b->g_info[g].w;
+    }
+    if (group_dst) group_dst[g] = b->g_dst[g];
+    if (group_members) {
+      group_members[2 * g] = b->g_mem[g].x;
+      group_members[2 * g + 1] = b->g_mem[g].y;
+    }
+  }
+  if (member_off) std::copy(b->m_off.begin(), b->m_off.end(), member_off);
+  if (member_shift) std::copy(b->m_shift.begin(), b->m_shift.end(), member_shift);
+  return 0;
+}
+
 int aosb_bloch_device_pattern(const aosb_bloch_t* b, const int64_t** indptr,
                               const int32_t** indices) {
   if (b == nullptr) return AOSB_ERR_NULL;

@@ -109,6 +109,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_bloch_upload": (C.c_int, [c_vp, C.c_char_p, c_sz]),
     "aosb_bloch_info": (C.c_int, [c_vp, C.POINTER(c_i64), C.POINTER(c_i64)]),
     "aosb_bloch_export": (C.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "aosb_bloch_export_groups": (C.c_int, [c_vp, C.POINTER(c_i64), C.POINTER(c_i64), c_vp, c_vp,
+                                           c_vp, c_vp, c_vp]),
     "aosb_bloch_device_pattern": (C.c_int, [c_vp, C.POINTER(c_vp), C.POINTER(c_vp)]),
     "aosb_bloch_apply": (C.c_int, [c_vp, c_i32, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp,
                                    C.c_char_p, c_sz]),

@@ -186,6 +186,18 @@ int aosb_bloch_info(const aosb_bloch_t *b, int64_t *nnz, int64_t *n_shifts);
  * shifts in lexicographic order), block_shift[n_blocks] (shift index). */
 int aosb_bloch_export(const aosb_bloch_t *b, int64_t *indptr, int32_t *indices,
                       int32_t *shifts, int32_t *block_shift);
+/* Host copies of the Bloch kernel's tables (no counterpart in the
+ * reference): per group of blocks with one atom pair (i, j), in
+ * (row atom, column atom) order, group_info[4g..4g+3] = (rows, columns, CSR
+ * row length of atom i, mirror group (j, i)), group_dst[g] = CSR position
+ * of the group's entry (0, 0), group_members[2g..2g+1] = [begin, end) of its
+ * member blocks; per member block, member_off = offset of its values and
+ * member_shift = its lattice-shift index.  Pass null arrays to read the
+ * counts first. */
+int aosb_bloch_export_groups(const aosb_bloch_t *b, int64_t *n_groups, int64_t *n_members,
+                             int32_t *group_info, int64_t *group_dst,
+                             int32_t *group_members, int64_t *member_off,
+                             int32_t *member_shift);
 /* Device CSR pattern arrays owned by the handle (valid until destroy). */
 int aosb_bloch_device_pattern(const aosb_bloch_t *b, const int64_t **indptr,
                               const int32_t **indices);

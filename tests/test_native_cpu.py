@@ -285,3 +285,81 @@ def test_row_blocks_share_columns_and_respect_the_cap(max_rows):
             first = indices[indptr[a]:indptr[a + 1]]
             for r in range(a + 1, z):
                 assert np.array_equal(indices[indptr[r]:indptr[r + 1]], first)
+
+
+def _emulate_bloch_windows(tables, values, ph, nnz):
+    """numpy restatement of bloch_windows_kernel's index mapping and float32
+    arithmetic (products without contraction, members added in block order,
+    the upper window's mean, its conjugate in the lower window)."""
+    info, dst, mem, moff, msh = tables
+    f32 = np.float32
+    zero, half = f32(0.0), f32(0.5)
+    out_r = np.zeros(nnz, f32)
+    out_i = np.zeros(nnz, f32)
+
+    def sums(rng, elem):
+        sr = si = None
+        for m in range(rng[0], rng[1]):
+            v = values[moff[m] + elem].astype(f32)
+            pr, pi = f32(ph[msh[m]].real), f32(ph[msh[m]].imag)
+            re, im = v * pr - zero * pi, v * pi + zero * pr
+            sr, si = (re, im) if sr is None else (sr + re, si + im)
+        return sr, si
+
+    for g in range(info.shape[0]):
+        nr, nc, rl, gm = (int(x) for x in info[g])
+        a = np.repeat(np.arange(nr), nc)
+        c = np.tile(np.arange(nc), nr)
+        pos = dst[g] + a * rl + c
+        if gm == g:
+            lo, hi = np.minimum(a, c), np.maximum(a, c)
+            xr, xi = sums(mem[g], lo * nc + hi)
+            yr, yi = sums(mem[g], hi * nc + lo)
+            mr_, mi_ = (xr + yr) * half, (xi - yi) * half
+            vr = np.where(a == c, xr, mr_)
+            vi = np.where(a == c, zero, np.where(a < c, mi_, -mi_))
+        else:
+            eg, em = a * nc + c, c * nr + a
+            lower = gm < g
+            xr, xi = sums(mem[gm] if lower else mem[g], em if lower else eg)
+            yr, yi = sums(mem[g] if lower else mem[gm], eg if lower else em)
+            vr, vi = (xr + yr) * half, (xi - yi) * half
+            if lower:
+                vi = -vi
+        out_r[pos] = vr
+        out_i[pos] = vi
+    out = np.empty(nnz, np.complex64)
+    out.real, out.imag = out_r, out_i
+    return out
+
+
+@pytest.mark.parametrize("name", ["small2d", "c1"])
+def test_bloch_window_kernel_emulation_matches_reference(name, golden):
+    """The device Bloch kernel's algorithm, replayed on the host from the
+    tables the library builds (aosb_bloch_export_groups), reproduces the
+    reference's H(k), S(k) bit for bit."""
+    b = getattr(bundles, name)()
+    rc, h, _ = _bloch_create(b)
+    assert rc == 0
+    lib = native.library()
+    try:
+        ng, nm = C.c_int64(), C.c_int64()
+        lib.aosb_bloch_export_groups(h, C.byref(ng), C.byref(nm), None, None, None, None, None)
+        info = np.empty((ng.value, 4), np.int32)
+        dst = np.empty(ng.value, np.int64)
+        mem = np.empty((ng.value, 2), np.int32)
+        moff = np.empty(nm.value, np.int64)
+        msh = np.empty(nm.value, np.int32)
+        lib.aosb_bloch_export_groups(h, C.byref(ng), C.byref(nm), info.ctypes.data,
+                                     dst.ctypes.data, mem.ctypes.data, moff.ctypes.data,
+                                     msh.ctypes.data)
+        pat = bloch_ref.build_pattern(b)
+        for k in bundles.KPOINTS[:2]:
+            ph = bloch_ref.phases(pat.shifts, k)
+            ref_h, ref_s = bloch_ref.bloch_pair(pat, b, k)
+            for vals, ref in ((b.operators.h_values, ref_h), (b.operators.s_values, ref_s)):
+                got = _emulate_bloch_windows((info, dst, mem, moff, msh), np.asarray(vals), ph,
+                                             ref.size)
+                assert np.array_equal(got, ref)
+    finally:
+        lib.aosb_bloch_destroy(h)
