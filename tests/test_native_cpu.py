@@ -363,3 +363,60 @@ def test_bloch_window_kernel_emulation_matches_reference(name, golden):
                 assert np.array_equal(got, ref)
     finally:
         lib.aosb_bloch_destroy(h)
+
+
+def _emulate_row_block_residual(rb, indptr, indices, h, s, pk, z, b, x, ncols, np_,
+                                warps=4):
+    """numpy restatement of row_block_kernel<R, residual>'s work split: CTA
+    index = (block, 32-column strip) * np + pencil; per CTA the block's
+    nonzeros are split between `warps` warps and their partial sums added."""
+    n = indptr.size - 1
+    r = np.full((np_, n, ncols), np.nan, np.complex128)
+    ncs = (ncols + 31) // 32
+    for cta in range((rb.size - 1) * ncs * np_):
+        p = cta % np_
+        bs = cta // np_
+        blk, strip = bs // ncs, bs % ncs
+        cols = np.arange(strip * 32, min(ncols, strip * 32 + 32))
+        r0, nr = rb[blk], rb[blk + 1] - rb[blk]
+        base0 = indptr[r0]
+        ln = indptr[r0 + 1] - base0
+        per = (ln + warps - 1) // warps
+        a = (h[pk[p]].astype(np.complex128) - z[p] * s[pk[p]].astype(np.complex128))
+        acc = np.zeros((nr, cols.size), np.complex128)
+        for w in range(warps):
+            w0, w1 = w * per, min(w * per + per, ln)
+            for q in range(nr):
+                seg = slice(base0 + q * ln + w0, base0 + q * ln + w1)
+                acc[q] += a[seg] @ x[p][indices[base0 + w0:base0 + w1]][:, cols]
+        r[p, r0:r0 + nr][:, cols] = b[p, r0:r0 + nr][:, cols] - acc
+    return r
+
+
+def test_row_block_residual_work_split_emulation():
+    """The row-block residual's CTA decode (pencil fastest), column strips and
+    warp split cover every (pencil, row, column) once and give b - (H - zS) x."""
+    from aospectrum_b200.engine import row_blocks
+    import scipy.sparse as sp
+
+    b_ = bundles.small2d()
+    pat = bloch_ref.build_pattern(b_)
+    k = bundles.KPOINTS[1]
+    hv, sv = bloch_ref.bloch_pair(pat, b_, k)
+    n = pat.indptr.size - 1
+    rb = row_blocks(pat.indptr, pat.indices, max_rows=13,
+                    starts=np.asarray(b_.basis.atom_offsets)[:-1])
+    rng = np.random.default_rng(3)
+    np_, ncols = 3, 40
+    x = rng.standard_normal((np_, n, ncols)) + 1j * rng.standard_normal((np_, n, ncols))
+    bb = rng.standard_normal((np_, n, ncols)) + 1j * rng.standard_normal((np_, n, ncols))
+    z = np.asarray([-2.0 + 0.1j, 0.5 + 0.01j, -1.0 + 1.0j])
+    pk = np.zeros(np_, np.int64)
+    got = _emulate_row_block_residual(rb, pat.indptr, pat.indices, hv[None], sv[None], pk, z,
+                                      bb, x, ncols, np_)
+    assert not np.isnan(got).any()
+    for p in range(np_):
+        a = sp.csr_matrix((hv.astype(np.complex128) - z[p] * sv.astype(np.complex128),
+                           pat.indices, pat.indptr), shape=(n, n))
+        ref = bb[p] - a @ x[p]
+        assert np.max(np.abs(got[p] - ref)) <= 1e-12 * np.max(np.abs(ref))
