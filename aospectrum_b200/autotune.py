@@ -148,6 +148,10 @@ def tune_batch(engine: Any, kpoints: Sequence[Sequence[float]], interval: Any,
     power-capped GPU moves between calls; one slow sample must not decide)."""
     import torch
 
+    def sync() -> None:
+        if torch.device(engine.device).type == "cuda":
+            torch.cuda.current_stream(engine.device).synchronize()
+
     st = engine.settings
     pairs = (st.integration_points + 1) // 2 if engine.engine.precision == "mixed" \
         else st.integration_points
@@ -160,10 +164,10 @@ def tune_batch(engine: Any, kpoints: Sequence[Sequence[float]], interval: Any,
     rates: dict[int, float] = {}
     for _ in range(max(1, repeats)):
         for s in sizes:
-            torch.cuda.current_stream(engine.device).synchronize()
+            sync()
             t0 = perf_counter()
             engine.solve_kpoints(kpoints[:s], interval)
-            torch.cuda.current_stream(engine.device).synchronize()
+            sync()
             rates[s] = max(rates.get(s, 0.0), s / (perf_counter() - t0))
     best = max(rates, key=rates.get)
     _BATCH_CACHE[key] = (best, rates)

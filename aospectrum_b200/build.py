@@ -31,29 +31,18 @@ def _nvcc() -> str:
     return found
 
 
-def _cutlass_include() -> list[str]:
-    import site
-
-    for root in site.getsitepackages():
-        cand = Path(root) / "flashinfer" / "data" / "cutlass" / "include"
-        if (cand / "cute" / "arch" / "mma_sm100_desc.hpp").exists():
-            return ["-I", str(cand)]
-    return []
-
-
 def build(verbose: bool = False, jobs: int | None = None) -> Path:
     nvcc = _nvcc()
     BUILD.mkdir(exist_ok=True)
     sources = sorted(CSRC.glob("*.cu"))
     headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
     newest_header = max((h.stat().st_mtime for h in headers), default=0.0)
-    extra = _cutlass_include()
 
     def compile_one(src: Path) -> Path:
         obj = BUILD / (src.stem + ".o")
         if obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, newest_header):
             return obj
-        cmd = [nvcc, *ARCH, *FLAGS, *extra, "-c", str(src), "-o", str(obj)]
+        cmd = [nvcc, *ARCH, *FLAGS, "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
         proc = subprocess.run(cmd, capture_output=True, text=True)

@@ -233,6 +233,17 @@ def nonspurious_mask(coefficients: np.ndarray, singular_values: np.ndarray,
     return np.isfinite(scores) & (scores >= threshold * top)
 
 
+def interval_mask(energies: np.ndarray, interval: EnergyInterval) -> np.ndarray:
+    """Strict interval test on the energies as the reference emits them:
+    cast to float32 first (``_rayleigh_ritz`` returns float32 energies,
+    ciss.py:145-150) and compared with the bounds as numpy compares a
+    float32 array with Python floats (ciss.py:355-358).  An FP64 energy a
+    float32 ulp inside a bound that rounds onto it is therefore dropped, as
+    the reference drops it."""
+    e32 = np.asarray(energies, dtype=np.float32)
+    return (e32 > interval.lower_ev) & (e32 < interval.upper_ev)
+
+
 def result_warnings(max_residual: float, saturated: bool) -> tuple[str, ...]:
     out = []
     if max_residual > 1.0e-3:

@@ -15,6 +15,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -39,12 +40,16 @@ uint64_t fnv1a(uint64_t h, const void* data, size_t bytes) {
   return h;
 }
 
+// The cached plan is shared: every call holds a reference for as long as it
+// uses the plan, so a concurrent call that replaces the cache entry (another
+// pattern or device) only drops the cache's reference, and the plan is
+// destroyed when the last call using it returns.
 struct PlanCache {
   std::mutex mu;
   int device = -1;
   int64_t n = 0, nnz = 0;
   uint64_t hash = 0;
-  aosb_plan* plan = nullptr;
+  std::shared_ptr<aosb_plan> plan;
 };
 PlanCache g_cache;
 
@@ -171,32 +176,35 @@ int aospectrum_b200_solve_complex64_ubatch_v1(const aospectrum_b200_ubatch_reque
   uint64_t h = 1469598103934665603ull;
   h = fnv1a(h, req->indptr, sizeof(int32_t) * (size_t)(n + 1));
   h = fnv1a(h, req->indices, sizeof(int32_t) * (size_t)nnz);
-  aosb_plan* plan = nullptr;
+  std::shared_ptr<aosb_plan> held;
   {
     std::lock_guard<std::mutex> lock(g_cache.mu);
-    if (g_cache.plan != nullptr && g_cache.device == dev && g_cache.n == n &&
-        g_cache.nnz == nnz && g_cache.hash == h) {
-      plan = g_cache.plan;
-    } else {
-      if (g_cache.plan != nullptr) aosb_plan_destroy(g_cache.plan);
-      g_cache.plan = nullptr;
-      std::vector<int64_t> ip(req->indptr, req->indptr + n + 1);
-      aosb_plan_options_v1 opt{AOSPECTRUM_B200_ABI_VERSION, sizeof(aosb_plan_options_v1),
-                               pick_tile(n), 1, 4 * pick_tile(n), 1};
-      int rc = aosb_plan_create(n, ip.data(), req->indices, nullptr, 0, &opt, &plan, em, ec);
-      if (rc != 0) return fail(rc);
-      rc = aosb_plan_upload(plan, em, ec);
-      if (rc != 0) {
-        aosb_plan_destroy(plan);
-        return fail(rc);
-      }
-      g_cache.plan = plan;
-      g_cache.device = dev;
-      g_cache.n = n;
-      g_cache.nnz = nnz;
-      g_cache.hash = h;
-    }
+    if (g_cache.plan && g_cache.device == dev && g_cache.n == n && g_cache.nnz == nnz &&
+        g_cache.hash == h)
+      held = g_cache.plan;
   }
+  if (!held) {
+    // analysis outside the lock; a call on another pattern may run meanwhile
+    std::vector<int64_t> ip(req->indptr, req->indptr + n + 1);
+    aosb_plan_options_v1 opt{AOSPECTRUM_B200_ABI_VERSION, sizeof(aosb_plan_options_v1),
+                             pick_tile(n), 1, 4 * pick_tile(n), 1};
+    aosb_plan* created = nullptr;
+    int rc = aosb_plan_create(n, ip.data(), req->indices, nullptr, 0, &opt, &created, em, ec);
+    if (rc != 0) return fail(rc);
+    rc = aosb_plan_upload(created, em, ec);
+    if (rc != 0) {
+      aosb_plan_destroy(created);
+      return fail(rc);
+    }
+    held = std::shared_ptr<aosb_plan>(created, [](aosb_plan* p) { aosb_plan_destroy(p); });
+    std::lock_guard<std::mutex> lock(g_cache.mu);
+    g_cache.plan = held;  // the previous entry lives on in the calls still holding it
+    g_cache.device = dev;
+    g_cache.n = n;
+    g_cache.nnz = nnz;
+    g_cache.hash = h;
+  }
+  aosb_plan* plan = held.get();
   res->analysis_seconds = now_seconds() - ta;
   res->reported_factor_nnz = plan->n_slots * plan->T * plan->T;
 

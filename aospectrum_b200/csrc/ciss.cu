@@ -257,6 +257,20 @@ size_t aosb_gram_scratch_bytes(int64_t n, int32_t p, int32_t q) {
   return (size_t)chunks * (size_t)p * (size_t)q * sizeof(double2);
 }
 
+namespace aosb {
+// The partial-sum grid is (ceil(p/32), ceil(q/32), ceil(n/512)); its y and z
+// extents are limited to 65535, so n above 33,553,920 rows (or q above
+// 2,097,120 columns) is rejected before anything is launched.
+static int gram_grid_check(int64_t n, int32_t q, char* err, size_t cap) {
+  const int64_t chunks = (n + kGramRows - 1) / kGramRows;
+  if (chunks > 65535 || ceil_div((int64_t)q, 32) > 65535)
+    return set_error(err, cap, AOSB_ERR_SIZE,
+                     "gram: n=%lld rows in %lld chunks of %d (or q=%d) exceeds the launch grid "
+                     "limit of 65535 chunks", (long long)n, (long long)chunks, kGramRows, q);
+  return 0;
+}
+}  // namespace aosb
+
 int aosb_gram(int64_t n, int32_t p, int32_t q, const aosb_complex128* x, int64_t ldx,
               const aosb_complex128* y, int64_t ldy, aosb_complex128* g, void* scratch,
               void* stream, char* err, size_t cap) {
@@ -264,6 +278,7 @@ int aosb_gram(int64_t n, int32_t p, int32_t q, const aosb_complex128* x, int64_t
     return aosb::set_error(err, cap, AOSB_ERR_NULL, "null argument");
   if (n <= 0 || p <= 0 || q <= 0 || ldx < p || ldy < q)
     return aosb::set_error(err, cap, AOSB_ERR_ARGUMENT, "invalid gram shape");
+  if (int rc = aosb::gram_grid_check(n, q, err, cap)) return rc;
   const int chunks = (int)((n + aosb::kGramRows - 1) / aosb::kGramRows);
   cudaStream_t st = (cudaStream_t)stream;
   dim3 grid(aosb::ceil_div(p, 32), aosb::ceil_div(q, 32), chunks);
@@ -331,6 +346,7 @@ extern "C" int aosb_gram_noalloc(int64_t n, int32_t p, int32_t q, const aosb_com
     return set_error(err, cap, AOSB_ERR_NULL, "null argument");
   if (n <= 0 || p <= 0 || q <= 0 || ldx < p || ldy < q)
     return set_error(err, cap, AOSB_ERR_ARGUMENT, "invalid gram shape");
+  if (int rc = gram_grid_check(n, q, err, cap)) return rc;
   const size_t need = aosb_gram_scratch_bytes(n, p, q);
   if (need > kNoAllocGramBytes)
     return set_error(err, cap, AOSB_ERR_SIZE,

@@ -9,6 +9,7 @@
 //               U_kj = inv(L_kk) P_k A_kj    (j > k, CTA owns column strips)
 //   3. schur:   A_ij -= L_ik U_kj            for every (i, j) target.
 // All kernels batch over pencils (grid.y / grid.x).
+#include <atomic>
 #include "plan.h"
 #include "cgemm.cuh"
 #include "factor.h"
@@ -485,14 +486,19 @@ __global__ void __launch_bounds__(kThreads) schur_kernel(int nU, const int32_t* 
 
 template <int T>
 int ensure_diag_attr(char* err, size_t cap) {
-  static bool done = false;
-  if (done) return 0;
+  // kernel attributes belong to each device's context: set once per device
+  // (devices past 63 set it on every call)
+  static std::atomic<uint64_t> attr_devices{0};
+  int device = 0;
+  cudaGetDevice(&device);
+  const uint64_t dev_bit = device < 64 ? (uint64_t)1 << device : 0;
+  if (dev_bit != 0 && (attr_devices.load() & dev_bit) != 0) return 0;
   const size_t diag_smem = diag_smem_bytes<T>();
   cudaError_t e = cudaFuncSetAttribute(diag_lu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)diag_smem);
   if (e != cudaSuccess)
     return set_error(err, cap, AOSB_ERR_CUDA, "diag_lu smem attribute: %s", cudaGetErrorString(e));
-  done = true;
+  attr_devices.fetch_or(dev_bit);
   return 0;
 }
 
@@ -517,11 +523,14 @@ void step_panels(const aosb_plan* P, const aosb_factor_args_v1* a, int64_t k) {
 }
 
 template <int T>
-int run_plain(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
+int run_plain(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap,
+              StepHook hook, void* hook_ctx) {
   cudaStream_t st = (cudaStream_t)a->stream;
   const int np = a->n_pencils;
   if (int rc = ensure_diag_attr<T>(err, cap)) return rc;
   for (int64_t k = 0; k < P->nb; ++k) {
+    if (hook != nullptr)
+      if (int rc = hook(hook_ctx, k, st, err, cap)) return rc;
     step_panels<T>(P, a, k);
     const int nL = P->lb_off[k + 1] - P->lb_off[k];
     const int nU = P->ur_off[k + 1] - P->ur_off[k];
@@ -577,11 +586,12 @@ int factor_step_diag(const aosb_plan* P, const aosb_factor_args_v1* a, int k, cu
   return 0;
 }
 
-int factor_plain(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
+int factor_plain(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap,
+                 StepHook hook, void* hook_ctx) {
   switch (P->T) {
-    case 32: return run_plain<32>(P, a, err, cap);
-    case 64: return run_plain<64>(P, a, err, cap);
-    case 128: return run_plain<128>(P, a, err, cap);
+    case 32: return run_plain<32>(P, a, err, cap, hook, hook_ctx);
+    case 64: return run_plain<64>(P, a, err, cap, hook, hook_ctx);
+    case 128: return run_plain<128>(P, a, err, cap, hook, hook_ctx);
   }
   return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "unsupported tile size");
 }

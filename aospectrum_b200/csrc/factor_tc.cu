@@ -211,6 +211,7 @@ struct PShared {
   uint64_t empty[kStagesP];
   uint64_t acc_full[2];
   uint64_t acc_empty[2];
+  uint64_t drain;  // the MMA issuer's last commit after a failure
   uint32_t tmem_base;
   int failed;
   // claimed item of the producer's j-th item (j % kItemRing), -1 = no more
@@ -324,7 +325,7 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     const ItemMap map, int n_pencils, int64_t n_slots, const unsigned char* __restrict__ staging,
     const unsigned char* __restrict__ staging1, int64_t staging_pencil_stride,
     int32_t* __restrict__ status, int* __restrict__ claim,
-    const __grid_constant__ CUtensorMap tmap_c) {
+    const __grid_constant__ CUtensorMap tmap_c, long long wl) {
   const int n_pairs = map.n_pairs;
   extern __shared__ unsigned char dyn[];
   PShared& sh = *reinterpret_cast<PShared*>(
@@ -340,9 +341,15 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
       mbar_init(&sh.acc_full[b], 1);
       mbar_init(&sh.acc_empty[b], kEpiWarps);
     }
+    mbar_init(&sh.drain, 1);
     sh.failed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  // What the producer and the MMA issuer have in flight, for the drain
+  // after a failure: the ring stages the producer filled (bit s) and the
+  // phase parity of its last fill of each; whether any MMA was issued.
+  uint32_t filled = 0, fill_parity = 0;
+  bool issued = false;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&sh.tmem_base)),
@@ -368,7 +375,7 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
           sh.items[j % kItemRing] = it;
           if (it < 0) {
             // stop token: one slab slot whose full[] completes without data
-            if (!mbar_wait(&sh.empty[stage], phase ^ 1)) {
+            if (!mbar_wait(&sh.empty[stage], phase ^ 1, wl)) {
               sh.failed = 1;
               atomicCAS(&status[0], 0, (int)AOSB_ERR_TIMEOUT);
               break;
@@ -387,11 +394,13 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
           const unsigned char* base = (bf[h] ? staging1 : staging) + (size_t)p * staging_pencil_stride;
           const unsigned char* stA = base + (size_t)ia[h] * kStagedTileBytes;
           const unsigned char* stB = base + (size_t)ib[h] * kStagedTileBytes;
-          if (!mbar_wait(&sh.empty[stage], phase ^ 1)) {
+          if (!mbar_wait(&sh.empty[stage], phase ^ 1, wl)) {
             sh.failed = 1;
             atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
             break;
           }
+          filled |= 1u << stage;
+          fill_parity = (fill_parity & ~(1u << stage)) | (phase << stage);
           mbar_expect_tx(&sh.full[stage], 2 * kOperandSlabBytes);
           bulk_g2s(sh.a[stage], stA + (size_t)sl * kOperandSlabBytes, kOperandSlabBytes,
                    &sh.full[stage]);
@@ -410,7 +419,7 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
       for (int j = 0; !sh.failed; ++j) {
         int it = blockIdx.x + j * (int)gridDim.x;
         if (claim == nullptr && it >= total) break;
-        if (!mbar_wait(&sh.acc_empty[acc], acc_phase ^ 1)) {
+        if (!mbar_wait(&sh.acc_empty[acc], acc_phase ^ 1, wl)) {
           sh.failed = 1;
           atomicCAS(&status[claim == nullptr ? it / n_pairs : 0], 0, (int)AOSB_ERR_TIMEOUT);
           break;
@@ -418,7 +427,7 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
         bool first_waited = false;
         if (claim != nullptr) {
           // the item index is published with the item's first slab
-          if (!mbar_wait(&sh.full[stage], phase)) {
+          if (!mbar_wait(&sh.full[stage], phase, wl)) {
             sh.failed = 1;
             atomicCAS(&status[0], 0, (int)AOSB_ERR_TIMEOUT);
             break;
@@ -437,11 +446,12 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
         const uint32_t re = tmem + (uint32_t)acc * 256, im = re + kTcT;
         bool ok = true;
         for (int s = 0; s < nslabs; ++s) {
-          if (!(s == 0 && first_waited) && !mbar_wait(&sh.full[stage], phase)) {
+          if (!(s == 0 && first_waited) && !mbar_wait(&sh.full[stage], phase, wl)) {
             ok = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          issued = true;
           const uint32_t sa = smem_u32(sh.a[stage]), sb = smem_u32(sh.b[stage]);
           uint64_t A[4], Bv[4];
 #pragma unroll
@@ -493,7 +503,8 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     for (int j = 0;; ++j) {
       int it = blockIdx.x + j * (int)gridDim.x;
       if (claim == nullptr && it >= total) break;
-      const bool ready = __all_sync(0xffffffffu, mbar_wait(&sh.acc_full[acc], acc_phase) ? 1 : 0);
+      const bool ready =
+          __all_sync(0xffffffffu, mbar_wait(&sh.acc_full[acc], acc_phase, wl) ? 1 : 0);
       if (!ready) {
         if (lane == 0) {
           sh.failed = 1;
@@ -554,6 +565,21 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     // the target updates must be complete (not only read) before exit
     if (lane == 0) bulk_wait_all();
     __syncwarp();
+  }
+  // Every role has left its loop (all waits are bounded).  After a failure
+  // the producer waits (bounded) until each stage it filled has received
+  // its bytes, and the MMA issuer commits once more and waits until its
+  // MMAs are done, so no copy or MMA lands in shared memory or TMEM after
+  // they are released.
+  __syncthreads();
+  if (sh.failed) {
+    if (warp == kEpiWarps && lane == 0)
+      for (int s = 0; s < kStagesP; ++s)
+        if (filled & (1u << s)) mbar_wait(&sh.full[s], (fill_parity >> s) & 1u);
+    if (warp == kEpiWarps + 1 && lane == 0 && issued) {
+      umma_commit(&sh.drain);
+      mbar_wait(&sh.drain, 0);
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -620,6 +646,15 @@ static int factor_tensor_map(void* factor, int64_t rows, CUtensorMap* map, char*
 // SMs left to the lookahead side stream (0 = the default rule); process-wide.
 std::atomic<int> g_lookahead_sms{0};
 
+// 1: the two-step Schur updates run as two-CTA pairs (schur_pair.cu);
+// process-wide.
+std::atomic<int> g_schur_pairs{0};
+
+// Polls of one mbarrier wait before a tensor-core kernel gives up and
+// records AOSB_ERR_TIMEOUT; process-wide, read at each launch.
+std::atomic<long long> g_tc_wait_limit{tc::kTcWaitLimit};
+long long tc::tc_wait_limit() { return g_tc_wait_limit.load(); }
+
 int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_t cap) {
   if (P->T != kTcT)
     return set_error(err, cap, AOSB_ERR_UNSUPPORTED, "tensor-core path needs tile = 128");
@@ -650,6 +685,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   if (int rc = factor_tensor_map(a->factor, (int64_t)np * P->n_slots * 2 * kTcT, &tmap_c, err, cap))
     return rc;
   const bool tc_panels = a->precision != AOSB_PRECISION_BF16X3_FP32_PANELS;
+  const long long wl = tc_wait_limit();
   auto grid_for = [&](int64_t items, int cap_ctas) {
     return (int)(items < cap_ctas ? items : cap_ctas);
   };
@@ -700,7 +736,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
         a->pivots, stage_buf(k), pencil_stride);
     const ItemMap pm{kMapPanel, nL, nU, nL + nU, 0, 0, nullptr, lslot, uslot, nullptr};
     schur_tc_kernel<<<grid_for((int64_t)(nL + nU) * np, cap_ctas), kPThreads, smem, s>>>(
-        pm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c);
+        pm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c, wl);
     count_launches(2);
     return 0;
   };
@@ -723,7 +759,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr,
                      nullptr};
     schur_tc_kernel<<<grid_for((int64_t)n_pairs * np, cap_ctas), kPThreads, smem, s>>>(
-        sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c);
+        sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c, wl);
     count_launches(1);
   };
   // Schur update of step k (the pairs `kind` selects) on the caller stream,
@@ -737,7 +773,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr,
                      nullptr};
     schur_tc_kernel<<<grid_for(items, cap_ctas), kPThreads, smem, st>>>(
-        sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c);
+        sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c, wl);
     count_launches(1);
     if (timed)
       timing_end(kTimedSchur, st, ev, (double)items * 8.0 * kTcT * kTcT * kTcT,
@@ -759,6 +795,8 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   // or the rest items, on stream s (timed); with `claim` the launch takes
   // items from the shared counter instead of a fixed share
   int* claim_counter = reinterpret_cast<int*>(staging + 4 * (int64_t)np * pencil_stride);
+  const bool pairs = g_schur_pairs.load() != 0 && P->d_sp_rest != nullptr;
+  int pair_rc = 0;
   auto two_step = [&](int64_t ss, bool cross, int cap_ctas, cudaStream_t s = nullptr,
                       int* claim = nullptr, bool count_work = true) {
     if (s == nullptr) s = st;
@@ -773,11 +811,23 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
       halves += (host[5 * i + 1] >= 0 ? 1 : 0) + (host[5 * i + 3] >= 0 ? 1 : 0);
     cudaEvent_t ev[2];
     const bool timed = count_work && timing_begin(s, ev);
-    const ItemMap lm{kMapList, 0, 0, (int)n, 0, 0, nullptr, nullptr, nullptr, dev + 5 * off[ss]};
-    schur_tc_kernel<<<grid_for(n * np, cap_ctas), kPThreads, smem, s>>>(
-        lm, np, P->n_slots, stage_buf(k0), stage_buf(k0 + 1), pencil_stride, a->status, claim,
-        tmap_c);
-    count_launches(1);
+    if (pairs) {
+      // the same items as pairs of targets sharing a column: two-CTA MMAs
+      const std::vector<int64_t>& poff = cross ? P->sp_cross_off : P->sp_rest_off;
+      const int32_t* pdev = cross ? P->d_sp_cross : P->d_sp_rest;
+      const int rc = schur_pair_launch(pdev + 8 * poff[ss], poff[ss + 1] - poff[ss], np,
+                                       P->n_slots, staging, 4 * buffer_bytes,
+                                       (k0 & 3) * buffer_bytes, ((k0 + 1) & 3) * buffer_bytes,
+                                       pencil_stride, a->status, claim, tmap_c, cap_ctas, s, err,
+                                       cap);
+      if (rc != 0 && pair_rc == 0) pair_rc = rc;
+    } else {
+      const ItemMap lm{kMapList, 0, 0, (int)n, 0, 0, nullptr, nullptr, nullptr, dev + 5 * off[ss]};
+      schur_tc_kernel<<<grid_for(n * np, cap_ctas), kPThreads, smem, s>>>(
+          lm, np, P->n_slots, stage_buf(k0), stage_buf(k0 + 1), pencil_stride, a->status, claim,
+          tmap_c, wl);
+      count_launches(1);
+    }
     // algorithmic bytes: every target read and written once, the staged L
     // and U tiles of both steps read once.  Of two launches sharing one
     // counter, the main one is timed with all the work: the second joins
@@ -832,6 +882,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
       } else {
         two_step(ss, false, sms);
       }
+      if (pair_rc != 0) return pair_rc;
     }
     return launch_check(err, cap, "tensor-core factorization");
   }
@@ -885,6 +936,16 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
 }
 
 }  // namespace aosb
+
+extern "C" int32_t aosb_factor_set_schur_pairs(int32_t on) {
+  if (on < 0 || on > 1) return -1;
+  return aosb::g_schur_pairs.exchange(on);
+}
+
+extern "C" int64_t aosb_tc_set_wait_limit(int64_t polls) {
+  if (polls < 0) return -1;
+  return aosb::g_tc_wait_limit.exchange(polls == 0 ? aosb::tc::kTcWaitLimit : polls);
+}
 
 extern "C" int32_t aosb_factor_set_lookahead_sms(int32_t sms) {
   if (sms < 0) return -1;

@@ -19,6 +19,8 @@
 
 #include <algorithm>
 #include <deque>
+#include <map>
+#include <tuple>
 #include <numeric>
 #include <vector>
 
@@ -241,6 +243,10 @@ void build_super_steps(aosb_plan* P) {
   P->ss_rest_off.assign(1, 0);
   P->ss_cross.clear();
   P->ss_rest.clear();
+  P->sp_cross_off.assign(1, 0);
+  P->sp_rest_off.assign(1, 0);
+  P->sp_cross.clear();
+  P->sp_rest.clear();
   struct Item {
     int32_t i, j, slot, a0, b0, a1, b1;
   };
@@ -294,6 +300,32 @@ void build_super_steps(aosb_plan* P) {
     }
     P->ss_cross_off.push_back((int64_t)P->ss_cross.size() / 5);
     P->ss_rest_off.push_back((int64_t)P->ss_rest.size() / 5);
+    // pairs: group each list's items by (column, halves present), pair them
+    // in row order, then order the pairs by (first row, column)
+    for (int list = 0; list < 2; ++list) {
+      std::map<std::tuple<int32_t, bool, bool>, std::vector<const Item*>> groups;
+      for (const Item& it : items) {
+        const bool cross = it.i == k2 || it.i == k3 || it.j == k2 || it.j == k3;
+        if (cross != (list == 0)) continue;
+        groups[std::make_tuple(it.j, it.a0 >= 0, it.a1 >= 0)].push_back(&it);
+      }
+      std::vector<std::pair<const Item*, const Item*>> pairs;
+      for (auto& g : groups)
+        for (size_t t = 0; t < g.second.size(); t += 2)
+          pairs.emplace_back(g.second[t], t + 1 < g.second.size() ? g.second[t + 1] : nullptr);
+      std::sort(pairs.begin(), pairs.end(), [](const auto& x, const auto& y) {
+        return x.first->i != y.first->i ? x.first->i < y.first->i : x.first->j < y.first->j;
+      });
+      std::vector<int32_t>& dst = list == 0 ? P->sp_cross : P->sp_rest;
+      for (const auto& pr : pairs) {
+        const Item& e = *pr.first;
+        const Item& o = pr.second ? *pr.second : *pr.first;
+        dst.insert(dst.end(), {e.slot, pr.second ? o.slot : -1, e.a0, o.a0, e.b0, e.a1, o.a1,
+                               e.b1});
+      }
+    }
+    P->sp_cross_off.push_back((int64_t)P->sp_cross.size() / 8);
+    P->sp_rest_off.push_back((int64_t)P->sp_rest.size() / 8);
   }
 }
 
@@ -301,7 +333,8 @@ void plan_free_device(aosb_plan* p) {
   int32_t** arrs[] = {&p->d_perm, &p->d_pinv, &p->d_slot, &p->d_lb_slot, &p->d_ur_slot,
                       &p->d_ua_slot, &p->d_ll_slot, &p->d_lb_tile, &p->d_ur_tile,
                       &p->d_ua_tile, &p->d_ll_tile, &p->d_sc_slot, &p->d_diag_slot,
-                      &p->d_indices, &p->d_ss_cross, &p->d_ss_rest};
+                      &p->d_indices, &p->d_ss_cross, &p->d_ss_rest, &p->d_sp_cross,
+                      &p->d_sp_rest};
   for (int32_t** a : arrs) {
     if (*a) cudaFree(*a);
     *a = nullptr;
@@ -584,6 +617,8 @@ int aosb_plan_upload(aosb_plan_t* P, char* err, size_t cap) {
   if (rc == 0) rc = aosb::up(&P->d_indptr, P->h_indptr, err, cap);
   if (rc == 0 && !P->ss_cross.empty()) rc = aosb::up(&P->d_ss_cross, P->ss_cross, err, cap);
   if (rc == 0 && !P->ss_rest.empty()) rc = aosb::up(&P->d_ss_rest, P->ss_rest, err, cap);
+  if (rc == 0 && !P->sp_cross.empty()) rc = aosb::up(&P->d_sp_cross, P->sp_cross, err, cap);
+  if (rc == 0 && !P->sp_rest.empty()) rc = aosb::up(&P->d_sp_rest, P->sp_rest, err, cap);
   if (rc == 0) rc = aosb::up(&P->d_indices, P->h_indices, err, cap);
   if (rc != 0) {
     aosb::plan_free_device(P);
@@ -635,6 +670,19 @@ int aosb_plan_export_super_steps(const aosb_plan_t* p, int64_t* n_super, int64_t
   if (rest_off) std::copy(p->ss_rest_off.begin(), p->ss_rest_off.end(), rest_off);
   if (cross) std::copy(p->ss_cross.begin(), p->ss_cross.end(), cross);
   if (rest) std::copy(p->ss_rest.begin(), p->ss_rest.end(), rest);
+  return 0;
+}
+
+int aosb_plan_export_pair_steps(const aosb_plan_t* p, int64_t* n_cross, int64_t* n_rest,
+                                int64_t* cross_off, int64_t* rest_off, int32_t* cross,
+                                int32_t* rest) {
+  if (p == nullptr) return AOSB_ERR_NULL;
+  if (n_cross) *n_cross = (int64_t)p->sp_cross.size() / 8;
+  if (n_rest) *n_rest = (int64_t)p->sp_rest.size() / 8;
+  if (cross_off) std::copy(p->sp_cross_off.begin(), p->sp_cross_off.end(), cross_off);
+  if (rest_off) std::copy(p->sp_rest_off.begin(), p->sp_rest_off.end(), rest_off);
+  if (cross) std::copy(p->sp_cross.begin(), p->sp_cross.end(), cross);
+  if (rest) std::copy(p->sp_rest.begin(), p->sp_rest.end(), rest);
   return 0;
 }
 

@@ -29,12 +29,24 @@ struct aosb_plan {
   // (read by the next super-step's panels), "rest" items elsewhere.
   std::vector<int64_t> ss_cross_off, ss_rest_off;  // [n_super + 1], in items
   std::vector<int32_t> ss_cross, ss_rest;
+  // The same items as pairs for the two-CTA (cta_group::2, M = 256) Schur
+  // update: two targets (i1, j), (i2, j) of one tile column with the same
+  // halves present share the B tiles; 8 ints per pair: target slot of the
+  // even CTA, of the odd CTA (-1 for a single: the odd CTA then computes a
+  // copy of the even CTA's product and discards it), then per step (2s, then
+  // 2s+1) the staged A index of the even CTA, of the odd CTA and the shared
+  // staged B index (all -1 when the step's half is absent).  Pairs are
+  // ordered by (first target row, column) so that neighbouring pairs share
+  // their A tiles.
+  std::vector<int64_t> sp_cross_off, sp_rest_off;  // [n_super + 1], in pairs
+  std::vector<int32_t> sp_cross, sp_rest;
   // Device copies.
   int32_t *d_perm = nullptr, *d_pinv = nullptr, *d_slot = nullptr;
   int32_t *d_lb_slot = nullptr, *d_ur_slot = nullptr, *d_ua_slot = nullptr, *d_ll_slot = nullptr;
   int32_t *d_lb_tile = nullptr, *d_ur_tile = nullptr, *d_ua_tile = nullptr, *d_ll_tile = nullptr;
   int32_t *d_sc_slot = nullptr, *d_diag_slot = nullptr;
   int32_t *d_ss_cross = nullptr, *d_ss_rest = nullptr;
+  int32_t *d_sp_cross = nullptr, *d_sp_rest = nullptr;
   // Pattern copies for the shifted-value assembly (host and device).
   std::vector<int64_t> h_indptr;
   std::vector<int32_t> h_indices;

@@ -85,6 +85,7 @@ struct SShared {
   uint64_t a_full[C::kAStages], a_empty[C::kAStages];
   uint64_t b_full[C::kBStages], b_empty[C::kBStages];
   uint64_t acc_full[2], acc_empty[2];
+  uint64_t drain;  // the MMA issuer's last commit after a failure
   uint32_t tmem_base;
   int failed;
 };
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
     const int32_t* __restrict__ slots, int64_t n_slots, float2* __restrict__ work,
     const float2* __restrict__ ytmp, const unsigned char* __restrict__ ystaged,
     int32_t* __restrict__ status, const __grid_constant__ CUtensorMap fmap,
-    const __grid_constant__ CUtensorMap xmap, int x_tma) {
+    const __grid_constant__ CUtensorMap xmap, int x_tma, long long wl) {
   const int strips = (nrhs + kNS - 1) / kNS;
   const int total = n_items * strips * n_pencils;
   const int work_ctas = (int)gridDim.x;
@@ -156,6 +157,7 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
       mbar_init(&sh.acc_full[b], 1);
       mbar_init(&sh.acc_empty[b], kEpiWarps);
     }
+    mbar_init(&sh.drain, 1);
     sh.failed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -169,6 +171,12 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = sh.tmem_base;
+  // What the producer and the MMA issuer have in flight, for the drain
+  // after a failure: the FP32-slab and Y-strip ring stages the producer
+  // filled (bit s) with the phase parity of the last fill of each, and
+  // whether any MMA was issued.
+  uint32_t raw_filled = 0, raw_parity = 0, b_filled = 0, b_parity = 0;
+  bool issued = false;
 
   if (warp == 0) {
     // ------------------------------------------------------------ producer
@@ -178,7 +186,12 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
       for (int it = blockIdx.x; it < total && !sh.failed; it += work_ctas, ++j) {
         const ItemOf w = item_of(it, n_items, strips);
         const int bb = j % kBStages;
-        if (!mbar_wait(&sh.b_empty[bb], (uint32_t)(((j / kBStages) & 1) ^ 1))) { fail(sh, status, w.p); break; }
+        if (!mbar_wait(&sh.b_empty[bb], (uint32_t)(((j / kBStages) & 1) ^ 1), wl)) {
+          fail(sh, status, w.p);
+          break;
+        }
+        b_filled |= 1u << bb;
+        b_parity = (b_parity & ~(1u << bb)) | ((uint32_t)((j / kBStages) & 1) << bb);
         mbar_expect_tx(&sh.b_full[bb], kSolveBBytes);
         bulk_g2s(sh.b[bb], ystaged + ((size_t)w.p * strips + w.strip) * kSolveBBytes,
                  kSolveBBytes, &sh.b_full[bb]);
@@ -186,10 +199,12 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
         bool ok = true;
         for (int s = 0; s < kSlabsS; ++s, ++g) {
           const int st = g % kRawStages;
-          if (!mbar_wait(&sh.raw_empty[st], (uint32_t)(((g / kRawStages) & 1) ^ 1))) {
+          if (!mbar_wait(&sh.raw_empty[st], (uint32_t)(((g / kRawStages) & 1) ^ 1), wl)) {
             ok = false;
             break;
           }
+          raw_filled |= 1u << st;
+          raw_parity = (raw_parity & ~(1u << st)) | ((uint32_t)((g / kRawStages) & 1) << st);
           mbar_expect_tx(&sh.raw_full[st], kRawBytes);
           if (OP == kOpPlain) {
             tma_load_2d(sh.raw[st][0], &fmap, s * kSK, (int)row0, &sh.raw_full[st]);
@@ -213,8 +228,8 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
         const int n16 = (ncols + 15) & ~15;
         const uint32_t id_pos = umma_idesc_mn(kT, n16, false), id_neg = umma_idesc_mn(kT, n16, true);
         const int acc = j & 1, bb = j % kBStages;
-        if (!mbar_wait(&sh.acc_empty[acc], (uint32_t)(((j >> 1) & 1) ^ 1)) ||
-            !mbar_wait(&sh.b_full[bb], (uint32_t)((j / kBStages) & 1))) {
+        if (!mbar_wait(&sh.acc_empty[acc], (uint32_t)(((j >> 1) & 1) ^ 1), wl) ||
+            !mbar_wait(&sh.b_full[bb], (uint32_t)((j / kBStages) & 1), wl)) {
           fail(sh, status, w.p);
           break;
         }
@@ -222,11 +237,12 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
         bool ok = true;
         for (int s = 0; s < kSlabsS; ++s, ++g) {
           const int ab = g % kAStages;
-          if (!mbar_wait(&sh.a_full[ab], (uint32_t)((g / kAStages) & 1))) {
+          if (!mbar_wait(&sh.a_full[ab], (uint32_t)((g / kAStages) & 1), wl)) {
             ok = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          issued = true;
           const uint32_t sa = smem_u32(sh.a[ab]), sb = smem_u32(sh.b[bb]) + s * kSolveBSlab;
           uint64_t A[4], Bv[4];
 #pragma unroll
@@ -262,8 +278,8 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
       bool ok = true;
       for (int s = 0; s < kSlabsS; ++s, ++g) {
         const int st = g % kRawStages, ab = g % kAStages;
-        const bool ready = mbar_wait(&sh.raw_full[st], (uint32_t)((g / kRawStages) & 1)) &&
-                           mbar_wait(&sh.a_empty[ab], (uint32_t)(((g / kAStages) & 1) ^ 1));
+        const bool ready = mbar_wait(&sh.raw_full[st], (uint32_t)((g / kRawStages) & 1), wl) &&
+                           mbar_wait(&sh.a_empty[ab], (uint32_t)(((g / kAStages) & 1) ^ 1), wl);
         if (!__all_sync(0xffffffffu, ready ? 1 : 0) || sh.failed) {
           ok = false;
           break;
@@ -347,7 +363,7 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
     for (int it = blockIdx.x; it < total; it += work_ctas, ++j) {
       const ItemOf w = item_of(it, n_items, strips);
       const int acc = j & 1;
-      const bool ready = mbar_wait(&sh.acc_full[acc], (uint32_t)((j >> 1) & 1));
+      const bool ready = mbar_wait(&sh.acc_full[acc], (uint32_t)((j >> 1) & 1), wl);
       if (!__all_sync(0xffffffffu, ready ? 1 : 0)) {
         if (lane == 0) fail(sh, status, w.p);
         break;
@@ -424,12 +440,24 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
     if (x_tma && lane == 0) bulk_wait_all();
     __syncwarp();
   }
-  // Every role has left its loop (all waits are bounded).  A CTA that
-  // stopped early pauses (bounded, ~0.2 ms) so that its own TMA loads and
-  // MMAs still in flight land before the shared memory and TMEM go away.
+  // Every role has left its loop (all waits are bounded).  After a failure
+  // the producer waits (bounded) until each stage it filled has received
+  // its bytes, and the MMA issuer commits once more and waits until its
+  // MMAs are done, so no copy or MMA lands in shared memory or TMEM after
+  // they are released.
   __syncthreads();
-  if (sh.failed && threadIdx.x == 0)
-    for (int i = 0; i < 200; ++i) __nanosleep(1000);
+  if (sh.failed) {
+    if (warp == 0 && lane == 0) {
+      for (int s = 0; s < kRawStages; ++s)
+        if (raw_filled & (1u << s)) mbar_wait(&sh.raw_full[s], (raw_parity >> s) & 1u);
+      for (int b = 0; b < kBStages; ++b)
+        if (b_filled & (1u << b)) mbar_wait(&sh.b_full[b], (b_parity >> b) & 1u);
+    }
+    if (warp == 1 && lane == 0 && issued) {
+      umma_commit(&sh.drain);
+      mbar_wait(&sh.drain, 0);
+    }
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
@@ -480,7 +508,7 @@ int solve_tc_launch(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
   dim3 g((unsigned)work_ctas);
   solve_tc_kernel<OP, CTAS><<<g, kSThreads, smem, st>>>(k, n, nrhs, np, P->n_pad, dtiles, dslots,
                                                         P->n_slots, work, ytmp, ystaged, status,
-                                                        fmap, xmap, x_tma);
+                                                        fmap, xmap, x_tma, tc_wait_limit());
   count_launches(1);
   return 0;
 }

@@ -13,9 +13,23 @@ namespace aosb {
 int encode_f32_2d(void* base, uint64_t inner, uint64_t rows, uint32_t box_x, uint32_t box_y,
                   bool swizzle128, CUtensorMap* map, char* err, size_t cap);
 
+// BF16 view of the split-BF16 staging buffer for the two-CTA Schur update:
+// [plane_slabs][2 K halves][2 operand-row halves][8 rows][64 elements]; a
+// box is one 16 KB A slab (four planes, both row halves) or, with half_b,
+// one 8 KB half of a B slab (four planes, one row half) (tma_map.cu).
+int encode_staging_5d(void* base, uint64_t plane_slabs, bool half_b, CUtensorMap* map, char* err,
+                      size_t cap);
+
 namespace tc {
 
-constexpr long long kTcWaitLimit = 1ll << 22;  // polls (with backoff) before timeout
+// Polls (with backoff) of one mbarrier wait before it gives up: the default
+// of the process-wide limit the kernels are launched with
+// (aosb_tc_set_wait_limit), and the fixed bound of the drain waits a CTA
+// makes on its own copies and MMAs after a failure.
+constexpr long long kTcWaitLimit = 1ll << 22;
+
+// Current process-wide wait limit (factor_tc.cu).
+long long tc_wait_limit();
 
 // B operand of the tensor-core solve update: one 32-column RHS strip of a
 // step's diagonal result Y (K = 128 rows) as four BF16 planes (re_hi,
@@ -44,10 +58,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
-// Bounded wait on phase `parity`; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait on phase `parity` (at most `limit` polls); returns false on
+// timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          long long limit = kTcWaitLimit) {
   const uint32_t addr = smem_u32(bar);
-  for (long long it = 0; it < kTcWaitLimit; ++it) {
+  for (long long it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"

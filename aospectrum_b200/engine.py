@@ -37,6 +37,7 @@ from .ciss import (
     CissSettings,
     EngineSettings,
     contour_geometry,
+    interval_mask,
     moment_coefficients,
     nonspurious_mask,
     probe_block,
@@ -431,6 +432,12 @@ class BandEngine:
         self.last_stats: dict[str, Any] = {}
         # optional device timing of every factorization call (CUDA events)
         self.profile_factor = False
+        # with keep_vectors, the last call's selected Ritz vectors (device
+        # complex128 [n][m] per k point, columns in the order of the
+        # returned energies) and their FP64 energies are kept
+        self.keep_vectors = False
+        self.last_vectors: list[Any] = []
+        self.last_energies: list[np.ndarray] = []
         self.factor_times_ms: list[float] = []
         self.factor_pencils: list[int] = []
 
@@ -772,16 +779,20 @@ class BandEngine:
         for k in range(nk):
             energies, coeffs = eig[k]
             keep = nonspurious_mask(coeffs, trunc[k][1], st.spurious_relative_threshold)
-            inside = (energies > interval.lower_ev) & (energies < interval.upper_ev)
+            inside = interval_mask(energies, interval)
             sel.append(np.flatnonzero(keep & inside))
         t = perf_counter()
         norms = [None] * nk
+        self.last_vectors = [None] * nk if self.keep_vectors else []
+        self.last_energies = [eig[k][0][sel[k]] for k in range(nk)] if self.keep_vectors else []
         for k in range(nk):
             if not sel[k].size:
                 continue
             energies, coeffs = eig[k]
             csel = torch.from_numpy(np.ascontiguousarray(coeffs[:, sel[k]])).to(dev)
             vec = self._dense_mul(basis[k], csel)
+            if self.keep_vectors:
+                self.last_vectors[k] = vec
             hv = torch.empty_like(vec)
             sv = torch.empty_like(vec)
             self._spmm(hvals[k], vec, hv)

@@ -91,6 +91,19 @@ class UbatchResult(C.Structure):
                 ("error_message", C.c_char * ERROR_CAPACITY)]
 
 
+class ShiftFactorStats(C.Structure):
+    _fields_ = [("upper_nnz", c_i64), ("factor_nnz", c_i64), ("pivot_count", c_i32),
+                ("inertia_positive", c_i32), ("inertia_negative", c_i32),
+                ("solve_calls", c_i32), ("solved_rhs", c_i64),
+                ("preparation_seconds", C.c_double), ("upload_seconds", C.c_double),
+                ("analysis_seconds", C.c_double), ("factorization_seconds", C.c_double),
+                ("solve_seconds", C.c_double), ("permanent_device_bytes", C.c_uint64),
+                ("peak_device_bytes", C.c_uint64), ("permanent_host_bytes", C.c_uint64),
+                ("peak_host_bytes", C.c_uint64),
+                ("free_device_bytes_before_factorization", C.c_uint64),
+                ("free_device_bytes_after_factorization", C.c_uint64)]
+
+
 # name: (restype, argtypes)
 _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_abi_version": (c_u32, []),
@@ -123,10 +136,14 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_plan_export_slots": (C.c_int, [c_vp, c_vp]),
     "aosb_plan_export_super_steps": (C.c_int, [c_vp, C.POINTER(c_i64), C.POINTER(c_i64),
                                                C.POINTER(c_i64), c_vp, c_vp, c_vp, c_vp]),
+    "aosb_plan_export_pair_steps": (C.c_int, [c_vp, C.POINTER(c_i64), C.POINTER(c_i64), c_vp,
+                                              c_vp, c_vp, c_vp]),
     "aosb_plan_destroy": (None, [c_vp]),
     "aosb_factor_bytes": (c_sz, [c_vp, c_i32]),
     "aosb_factor_workspace_bytes": (c_sz, [c_vp, c_i32, c_i32]),
     "aosb_factor_set_lookahead_sms": (c_i32, [c_i32]),
+    "aosb_tc_set_wait_limit": (c_i64, [c_i64]),
+    "aosb_factor_set_schur_pairs": (c_i32, [c_i32]),
     "aosb_solve_set_ctas_per_sm": (c_i32, [c_i32]),
     "aosb_factor": (C.c_int, [c_vp, C.POINTER(FactorArgs), C.c_char_p, c_sz]),
     "aosb_solve": (C.c_int, [c_vp, C.POINTER(SolveArgs), C.c_char_p, c_sz]),
@@ -152,6 +169,15 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
                             C.c_char_p, c_sz]),
     "aosb_gram_noalloc": (C.c_int, [c_i64, c_i32, c_i32, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp,
                                     C.c_char_p, c_sz]),
+    "aosb_shift_factor_create_device": (C.c_int, [C.POINTER(c_vp), c_i64, c_i64, c_vp, c_vp,
+                                                  c_vp, c_vp, C.c_float, c_i32, c_vp,
+                                                  C.c_char_p, c_sz]),
+    "aosb_shift_factor_refactor_device": (C.c_int, [c_vp, c_vp, c_vp, C.c_float, C.c_char_p,
+                                                    c_sz]),
+    "aosb_shift_factor_solve": (C.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, c_i32, C.c_char_p,
+                                          c_sz]),
+    "aosb_shift_factor_get_stats": (None, [c_vp, C.POINTER(ShiftFactorStats)]),
+    "aosb_shift_factor_destroy": (None, [c_vp]),
     "aosb_dense_mul": (C.c_int, [c_i64, c_i32, c_i32, c_vp, c_i64, c_vp, c_vp, c_i64, c_vp,
                                  C.c_char_p, c_sz]),
     "aosb_column_norms": (C.c_int, [c_i64, c_i32, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp,

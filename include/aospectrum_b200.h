@@ -267,6 +267,15 @@ int aosb_plan_export_slots(const aosb_plan_t *plan, int32_t *slot);
 int aosb_plan_export_super_steps(const aosb_plan_t *plan, int64_t *n_super, int64_t *n_cross,
                                  int64_t *n_rest, int64_t *cross_off, int64_t *rest_off,
                                  int32_t *cross, int32_t *rest);
+/* The same items as pairs for the two-CTA (M = 256) Schur update, host
+ * copies for inspection and tests; no counterpart in the reference.  Pairs
+ * of 8 ints: target slot of the even CTA, of the odd CTA (-1: single),
+ * then for step 2s and step 2s+1 the staged A index of the even CTA, of the
+ * odd CTA and the shared staged B index (-1 when that step's half is
+ * absent).  cross_off / rest_off hold [n_super + 1] pair offsets. */
+int aosb_plan_export_pair_steps(const aosb_plan_t *plan, int64_t *n_cross, int64_t *n_rest,
+                                int64_t *cross_off, int64_t *rest_off, int32_t *cross,
+                                int32_t *rest);
 void aosb_plan_destroy(aosb_plan_t *plan);
 
 /* ------------------------------------------------------------------------
@@ -318,6 +327,22 @@ int aosb_factor(const aosb_plan_t *plan, const aosb_factor_args_v1 *args,
  * Process-wide; returns the previous setting (-1 for sms < 0).  No
  * counterpart in the reference (cuDSS schedules internally). */
 int32_t aosb_factor_set_lookahead_sms(int32_t sms);
+/* 1: the two-step tensor-core Schur updates run as pairs of targets of one
+ * tile column on two-CTA clusters (tcgen05 cta_group::2, M = 256: the pair
+ * shares the B operand, a quarter less operand traffic per MMA); 0: one
+ * target per CTA.  Process-wide; returns the previous setting (-1 for
+ * other values).  No counterpart in the reference. */
+int32_t aosb_factor_set_schur_pairs(int32_t on);
+/* Polls of one mbarrier wait in the tensor-core kernels (factorization
+ * Schur/panel products and solve updates) before the waiting CTA gives up:
+ * it records AOSB_ERR_TIMEOUT in the pencil's status word, waits (with the
+ * default bound) for its own copies and MMAs in flight, frees its TMEM and
+ * returns, so the context stays usable.  The default is 4,194,304 polls
+ * with backoff (well over a second of waiting); 0 restores it.
+ * Process-wide, read at each launch; returns the previous value (-1 for a
+ * negative argument).  No counterpart in the reference (cuDSS has no
+ * bounded waits to set). */
+int64_t aosb_tc_set_wait_limit(int64_t polls);
 
 /* ------------------------------------------------------------------------
  * Block-RHS triangular solves in the permuted, padded order:
@@ -456,6 +481,68 @@ int aosb_dense_mul(int64_t n, int32_t p, int32_t r, const aosb_complex128 *x,
 int aosb_column_norms(int64_t n, int32_t m, const aosb_complex128 *a,
                       const aosb_complex128 *b, int64_t ld, const double *e,
                       double *out, void *stream, char *err, size_t err_cap);
+
+/* ------------------------------------------------------------------------
+ * Real symmetric shifted factorization with inertia (Gamma point).
+ * Replaces aospectrum_cudss_shift_factor_{create_device,refactor_device,
+ * solve,get_stats,destroy} (native/include/aospectrum_cudss_shift_factor.h:
+ * 15-76, native/src/aospectrum_cudss_shift_factor.c:232-742): same
+ * arguments in the same order, the same statistics block, and the same
+ * meaning -- A = H - shift * S from the upper triangle (diagonal included)
+ * of the caller's real float32 CSR values on the DEVICE, int32 CSR pattern
+ * on the host; inertia_negative / inertia_positive count the eigenvalues of
+ * the pencil (H, S) below / above the shift (S positive definite), so
+ * n - negative - positive is the count at the shift.  Differences: the
+ * factorization is this library's tile block elimination (FP32 tile
+ * updates, partial pivoting inside diagonal tiles) with the inertia taken
+ * tile by tile from a Bunch-Kaufman LDL^T of each eliminated diagonal tile;
+ * pivot_count is the number of symmetric interchanges those LDL^Ts made;
+ * factor_nnz counts the stored tile entries.  Functions return 0 or an
+ * AOSB_ERR_* status (the reference returns 1 for every failure); a shift at
+ * which a diagonal tile is exactly singular fails with AOSB_ERR_DEVICE_INFO.
+ * rhs / solution of aosb_shift_factor_solve are device float32 column-major
+ * blocks (leading dimension >= n), as the reference's PRIMME preconditioner
+ * passes them; the call synchronizes the stream.
+ * ------------------------------------------------------------------------ */
+typedef struct aosb_shift_factor aosb_shift_factor_t;
+
+typedef struct {
+  int64_t upper_nnz;
+  int64_t factor_nnz;
+  int32_t pivot_count;
+  int32_t inertia_positive;
+  int32_t inertia_negative;
+  int32_t solve_calls;
+  int64_t solved_rhs;
+  double preparation_seconds;
+  double upload_seconds;
+  double analysis_seconds;
+  double factorization_seconds;
+  double solve_seconds;
+  uint64_t permanent_device_bytes;
+  uint64_t peak_device_bytes;
+  uint64_t permanent_host_bytes;
+  uint64_t peak_host_bytes;
+  uint64_t free_device_bytes_before_factorization;
+  uint64_t free_device_bytes_after_factorization;
+} aosb_shift_factor_stats;
+
+int aosb_shift_factor_create_device(aosb_shift_factor_t **factor, int64_t n, int64_t nnz,
+                                    const int32_t *indptr, const int32_t *indices,
+                                    const float *device_hamiltonian_values,
+                                    const float *device_overlap_values, float shift,
+                                    int32_t maximum_rhs, void *stream, char *err,
+                                    size_t err_cap);
+int aosb_shift_factor_refactor_device(aosb_shift_factor_t *factor,
+                                      const float *device_hamiltonian_values,
+                                      const float *device_overlap_values, float shift,
+                                      char *err, size_t err_cap);
+int aosb_shift_factor_solve(aosb_shift_factor_t *factor, const float *rhs,
+                            int64_t leading_rhs, float *solution, int64_t leading_solution,
+                            int32_t rhs_count, char *err, size_t err_cap);
+void aosb_shift_factor_get_stats(const aosb_shift_factor_t *factor,
+                                 aosb_shift_factor_stats *stats);
+void aosb_shift_factor_destroy(aosb_shift_factor_t *factor);
 
 #ifdef __cplusplus
 }

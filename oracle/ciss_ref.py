@@ -83,8 +83,23 @@ def solve_interval(h: sparse.csr_matrix, s: sparse.csr_matrix, lower: float, upp
     mom = np.zeros((n, block * moments), dtype=np.complex64)
     for j in range(n_points):
         x = shifted_solve(h, s, shifts[j], rhs, method)
-        for m in range(moments):
-            mom[:, m * block:(m + 1) * block] += -weights[j] * nodes[j] ** m * x
+        accumulate_moments(mom, x, weights[j], nodes[j], block, moments)
+    return subspace(h, s, mom, lower, upper, block=block, moments=moments, rank_tol=rank_tol,
+                    ghost_tol=ghost_tol)
+
+
+def accumulate_moments(mom: np.ndarray, x: np.ndarray, weight, node, block: int,
+                       moments: int) -> None:
+    """mom[:, m L:(m+1) L] += -w_j zeta_j^m X_j in complex64 (ciss.py:324-333)."""
+    for m in range(moments):
+        mom[:, m * block:(m + 1) * block] += -weight * node ** m * x
+
+
+def subspace(h: sparse.csr_matrix, s: sparse.csr_matrix, mom: np.ndarray, lower: float,
+             upper: float, *, block: int, moments: int, rank_tol: float = 1.0e-5,
+             ghost_tol: float = 1.0e-4) -> RefCissResult:
+    """Compression, Rayleigh-Ritz, ghost filter, selection and residuals of
+    the moment block (ciss.py:107-177, :334-372)."""
     gram = mom.conj().T @ (s @ mom)
     gram = 0.5 * (gram + gram.conj().T)
     lam, vec = np.linalg.eigh(gram)

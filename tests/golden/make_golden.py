@@ -1,7 +1,9 @@
 """Generates the golden vectors under tests/golden/ from the REFERENCE itself.
 
-Run in a container where the reference sources are mounted:
-    python tests/golden/make_golden.py /root/reference
+Run in a container where the reference sources are available, passing
+their root (the directory holding src/aospectrum and examples/):
+    python tests/golden/make_golden.py REFERENCE_ROOT
+    python tests/golden/make_golden.py REFERENCE_ROOT --c2 0,37
 
 It imports the reference's Python package (yumiaoyi-o/AOSpectrum,
 src/aospectrum) and records, for seeded bundles written by
@@ -15,6 +17,15 @@ aospectrum_b200.write_bundle and read back by the reference's load_bundle:
   * read_kpath on the reference's example k path;
   * the bands.csv / summary.json of the reference's run_band on a tiny
     bundle (same injected solver).
+With ``--c2 K1,K2,...`` only the 1000-atom c2 workload is recorded
+(tests/golden/c2.npz and manifest_c2.json): the reference's Bloch digests at
+those k-path indices, FP64 dense generalized eigenvalues of the same H(k),
+S(k) in the solve interval, and the reference's complex64 CISS
+(solve_interval) with exact complex128 dense-LU shifted solves injected
+through its shifted_solver seam: its eigenvalues and maximum residual.  One
+LU of H - z S serves the node z and its conjugate partner, since
+(H - z S)^H = H - conj(z) S for Hermitian H, S.  This takes tens of minutes
+of host time (16 dense LUs of n = 13000 per k point).
 The reference's cuDSS extension is not importable here and is not needed.
 """
 
@@ -190,5 +201,96 @@ def main(reference_root: str) -> None:
     print("golden vectors written to", HERE)
 
 
+def main_c2(reference_root: str, kidx: list[int]) -> None:
+    import time
+
+    sys.path.insert(0, str(Path(reference_root) / "src"))
+    from aospectrum.bundle import load_bundle
+    from aospectrum.ciss import CissSettings, CudssCissSolver, ShiftedResult
+    from aospectrum.data import EnergyInterval
+    from aospectrum.sparse import BlochPattern
+    from scipy import linalg
+
+    from aospectrum_b200 import synth
+    from aospectrum_b200.kpath import kpath_from_dict
+
+    class DenseShifted:
+        """Exact complex128 dense-LU shifted solves; the LU of node z also
+        solves its conjugate partner with the conjugate transpose."""
+
+        def __init__(self):
+            self.cache: dict[complex, np.ndarray] = {}
+            self.factorizations = 0
+
+        def solve_shifted(self, matrices, shifts, rhs):
+            out = np.empty((shifts.size,) + rhs.shape, dtype=np.complex64)
+            b = rhs.astype(np.complex128)
+            for i, z in enumerate(shifts):
+                z = complex(z)
+                if z in self.cache:
+                    out[i] = self.cache.pop(z)
+                    continue
+                a = matrices.hamiltonian.toarray().astype(np.complex128)
+                a -= z * matrices.overlap.toarray().astype(np.complex128)
+                lu = linalg.lu_factor(a, overwrite_a=True, check_finite=False)
+                del a
+                self.factorizations += 1
+                out[i] = linalg.lu_solve(lu, b, check_finite=False)
+                self.cache[z.conjugate()] = linalg.lu_solve(lu, b, trans=2, check_finite=False)
+            return ShiftedResult(out, {}, None)
+
+        def close(self):
+            pass
+
+    w = synth.WORKLOADS["c2"]
+    kp = kpath_from_dict(w.kpath)
+    guard = 0.02
+    lo, hi = w.window_ev[0] - guard, w.window_ev[1] + guard
+    tmp = Path(tempfile.mkdtemp())
+    my_bundle.write_bundle(synth.generate_bundle(w.spec), tmp / "c2")
+    rb = load_bundle(tmp / "c2")
+    pat = BlochPattern.from_bundle(rb)
+    ws = pat.workspace(complex_values=True)
+    manifest = {"generator": "tests/golden/make_golden.py --c2", "workload": "c2",
+                "interval": [lo, hi], "nnz": int(pat.nnz),
+                "indptr": sha(np.asarray(pat.csr_indptr)),
+                "indices": sha(np.asarray(pat.csr_indices)), "kpoints": {}}
+    arrays = {}
+    for i in kidx:
+        t0 = time.perf_counter()
+        pair = ws.update(rb, kp.fractional_points[i])
+        rec = {"k": [float(v) for v in kp.fractional_points[i]],
+               "h": sha(pair.hamiltonian.data), "s": sha(pair.overlap.data)}
+        h = pair.hamiltonian.toarray().astype(np.complex128)
+        s_ = pair.overlap.toarray().astype(np.complex128)
+        exact = linalg.eigh(0.5 * (h + h.conj().T), 0.5 * (s_ + s_.conj().T),
+                            eigvals_only=True, subset_by_value=(lo, hi), check_finite=False)
+        del h, s_
+        arrays[f"k{i}_fp64"] = np.sort(exact)
+        shim = DenseShifted()
+        res = CudssCissSolver(CissSettings(), shifted_solver=shim).solve_interval(
+            pair, EnergyInterval(lo, hi))
+        arrays[f"k{i}_energies"] = np.asarray(res.energies_ev)
+        rec.update({"max_residual_ev": res.maximum_residual_ev, "complete": res.complete,
+                    "count": int(res.energies_ev.size), "fp64_count": int(exact.size),
+                    "factorizations": shim.factorizations,
+                    "seconds": round(time.perf_counter() - t0, 1)})
+        manifest["kpoints"][str(i)] = rec
+        print("c2 k", i, rec, flush=True)
+    np.savez_compressed(HERE / "c2.npz", **arrays)
+    (HERE / "manifest_c2.json").write_text(json.dumps(manifest, indent=2, sort_keys=True) + "\n")
+    shutil.rmtree(tmp)
+    print("c2 golden vectors written to", HERE)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import argparse
+
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("reference_root", help="root of the reference sources")
+    ap.add_argument("--c2", default="", help="record only c2 at these k-path indices")
+    a = ap.parse_args()
+    if a.c2:
+        main_c2(a.reference_root, [int(v) for v in a.c2.split(",")])
+    else:
+        main(a.reference_root)

@@ -181,3 +181,21 @@ def test_parallel_small_eigensolves_match_serial():
         eng._host_map(lambda g: truncate_gram(g, 1e-5, limit_threads=False),
                       [grams[0], np.zeros((24, 24), complex)])
     eng._lapack_pool.shutdown()
+
+
+def test_interval_selection_uses_float32_energies():
+    """The reference casts the Ritz energies to float32 before its strict
+    interval test (ciss.py:145-150, :355-358): an FP64 energy that lies a
+    hair inside a bound but rounds onto it in float32 is dropped, and no
+    kept energy equals a bound."""
+    from aospectrum_b200.ciss import interval_mask
+
+    iv = EnergyInterval(-2.5, -1.0)
+    e = np.array([-2.5 + 1e-9, -2.0, -1.0 - 1e-9, -1.0 - 1e-6])
+    got = interval_mask(e, iv)
+    e32 = np.asarray(e, dtype=np.float32)
+    ref = np.logical_and(e32 > iv.lower_ev, e32 < iv.upper_ev)
+    assert np.array_equal(got, ref)
+    assert got.tolist() == [False, True, False, True]
+    kept = np.asarray(e[got], dtype=np.float32)
+    assert not np.any(kept == np.float32(iv.lower_ev)) and not np.any(kept == np.float32(iv.upper_ev))

@@ -190,6 +190,73 @@ def test_two_step_schur_lists_cover_both_steps(name, tile, ordering):
     lib.aosb_plan_destroy(h)
 
 
+@pytest.mark.parametrize("name,tile,ordering", [("c1", 32, 1), ("c1", 64, 0), ("small2d", 32, 0),
+                                                ("c1", 128, 0)])
+def test_pair_lists_hold_the_two_step_items_in_column_pairs(name, tile, ordering):
+    """The two-CTA pair lists: every two-step item appears exactly once, as
+    the even or odd member of a pair; the two members of a pair share their
+    tile column, the B index and which halves are present; a single has odd
+    slot -1 and repeats the even member's A indices; pairs are ordered by
+    (first row, column)."""
+    b = getattr(bundles, name)()
+    pat = bloch_ref.build_pattern(b)
+    rc, h, msg = _plan(pat.indptr, pat.indices, b.n_orbitals, tile, ordering,
+                       np.ascontiguousarray(b.basis.atom_offsets, np.int64))
+    assert rc == 0, msg
+    lib = native.library()
+    info = native.PlanInfo()
+    lib.aosb_plan_info(h, C.byref(info))
+    nb = info.n_tiles
+    slot = np.empty(nb * nb, np.int32)
+    lib.aosb_plan_export_slots(h, slot.ctypes.data)
+    where = {int(v): divmod(q, nb) for q, v in enumerate(slot) if v >= 0}
+    ns, nc, nr = C.c_int64(), C.c_int64(), C.c_int64()
+    lib.aosb_plan_export_super_steps(h, C.byref(ns), C.byref(nc), C.byref(nr), None, None, None,
+                                     None)
+    coff = np.empty(ns.value + 1, np.int64)
+    roff = np.empty(ns.value + 1, np.int64)
+    cross = np.empty(5 * max(nc.value, 1), np.int32)
+    rest = np.empty(5 * max(nr.value, 1), np.int32)
+    lib.aosb_plan_export_super_steps(h, None, None, None, coff.ctypes.data, roff.ctypes.data,
+                                     cross.ctypes.data, rest.ctypes.data)
+    pc, pr = C.c_int64(), C.c_int64()
+    lib.aosb_plan_export_pair_steps(h, C.byref(pc), C.byref(pr), None, None, None, None)
+    pcoff = np.empty(ns.value + 1, np.int64)
+    proff = np.empty(ns.value + 1, np.int64)
+    pcross = np.empty(8 * max(pc.value, 1), np.int32)
+    prest = np.empty(8 * max(pr.value, 1), np.int32)
+    lib.aosb_plan_export_pair_steps(h, None, None, pcoff.ctypes.data, proff.ctypes.data,
+                                    pcross.ctypes.data, prest.ctypes.data)
+    pairs_total = singles = 0
+    for items, off, pitems, poff in ((cross, coff, pcross, pcoff), (rest, roff, prest, proff)):
+        for s in range(ns.value):
+            want = {int(it[0]): tuple(int(v) for v in it[1:])
+                    for it in items[5 * off[s]:5 * off[s + 1]].reshape(-1, 5)}
+            got = {}
+            prev = None
+            for p in pitems[8 * poff[s]:8 * poff[s + 1]].reshape(-1, 8):
+                e, o, a0e, a0o, b0, a1e, a1o, b1 = (int(v) for v in p)
+                got[e] = (a0e, b0, a1e, b1)
+                ie, je = where[e]
+                if o >= 0:
+                    io, jo = where[o]
+                    assert jo == je and io > ie
+                    got[o] = (a0o, b0, a1o, b1)
+                    assert (a0o >= 0) == (a0e >= 0) and (a1o >= 0) == (a1e >= 0)
+                else:
+                    singles += 1
+                    assert (a0o, a1o) == (a0e, a1e)
+                key = (ie, je)
+                assert prev is None or key > prev
+                prev = key
+                pairs_total += 1
+            assert got == want, s
+    assert pairs_total > 0
+    # most items pair up
+    assert singles < 0.5 * pairs_total
+    lib.aosb_plan_destroy(h)
+
+
 def test_symbolic_plan_rejects_bad_patterns():
     ip = np.array([0, 2, 3], np.int64)
     assert _plan(ip, np.array([0, 1, 0], np.int32), 2)[0] == 33      # row 1 misses its diagonal
@@ -234,6 +301,21 @@ def test_ubatch_request_validation_codes():
     assert rc != 0 and res.status == 35 and b"non-finite" in res.error_message
 
 
+def test_gram_rejects_row_counts_beyond_the_launch_grid():
+    """Both Gram entry points split n into 512-row chunks on the grid's z
+    axis (at most 65535): a larger n is rejected with status 34 before any
+    launch, so no pointer is touched (these are never dereferenced)."""
+    lib = native.library()
+    fake = 1 << 20
+    n = 65536 * 512   # one chunk too many; p = q = 1 fits the no-alloc scratch
+    buf = C.create_string_buffer(512)
+    rc = lib.aosb_gram(n, 1, 1, fake, 1, fake, 1, fake, fake, None, buf, 512)
+    assert rc == 34 and b"65535" in buf.value
+    buf = C.create_string_buffer(512)
+    rc = lib.aosb_gram_noalloc(n, 1, 1, fake, 1, fake, 1, fake, None, buf, 512)
+    assert rc == 34 and b"65535" in buf.value
+
+
 def test_shift_session_argument_checks():
     from aospectrum_b200.solvers import B200ShiftSession
 
@@ -265,6 +347,14 @@ def test_process_wide_tuning_setters_round_trip():
     assert lib.aosb_solve_set_ctas_per_sm(0) == 1
     assert lib.aosb_solve_set_ctas_per_sm(3) == -1
     assert lib.aosb_solve_set_ctas_per_sm(prev) == 2   # 0 restored the default, 2
+    prev = lib.aosb_factor_set_schur_pairs(1)
+    assert lib.aosb_factor_set_schur_pairs(prev) == 1
+    assert lib.aosb_factor_set_schur_pairs(2) == -1
+    prev = lib.aosb_tc_set_wait_limit(7)
+    assert prev == 1 << 22
+    assert lib.aosb_tc_set_wait_limit(0) == 7
+    assert lib.aosb_tc_set_wait_limit(-3) == -1
+    assert lib.aosb_tc_set_wait_limit(prev) == 1 << 22
 
 
 @pytest.mark.parametrize("max_rows", [4, 13, 16])
