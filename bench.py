@@ -69,6 +69,8 @@ def parse() -> argparse.Namespace:
                     help="tile steps per tensor-core Schur pass (2 = K 256)")
     ap.add_argument("--lookahead-sms", type=int, default=0,
                     help="SMs left to the factorization's lookahead side stream (0 = default)")
+    ap.add_argument("--schur-pairs", type=int, default=-1, choices=(-1, 0, 1),
+                    help="two-CTA (M = 256) pair Schur updates: 1 on, 0 off, -1 library default")
     ap.add_argument("--solve-ctas", type=int, default=0, choices=(0, 1, 2),
                     help="CTAs per SM of the tensor-core solve update (0 = default)")
     ap.add_argument("--tensor-core-solves", type=int, default=-1,
@@ -537,6 +539,10 @@ def main() -> None:
         native.library().aosb_factor_set_lookahead_sms(args.lookahead_sms)
     if args.solve_ctas:
         native.library().aosb_solve_set_ctas_per_sm(args.solve_ctas)
+    if args.schur_pairs >= 0:
+        native.library().aosb_factor_set_schur_pairs(args.schur_pairs)
+    pairs_on = native.library().aosb_factor_set_schur_pairs(0)
+    native.library().aosb_factor_set_schur_pairs(pairs_on)
     w, kp = workload(args.workload)
     bundle = synth.generate_bundle(w.spec)
     interval = EnergyInterval(w.window_ev[0] - GUARD_EV, w.window_ev[1] + GUARD_EV)
@@ -697,6 +703,7 @@ def main() -> None:
                    else 0,
                    "tensor_core_solves": bool(eng.engine.tensor_core_solves),
                    "schur_depth": eng.engine.schur_depth,
+                   "schur_pairs": bool(pairs_on),
                    "lookahead_sms": args.lookahead_sms or "default",
                    "solve_ctas_per_sm": args.solve_ctas or "default",
                    "autotune": tuning,
