@@ -313,16 +313,30 @@ class ServingRequestSpec:
     arrival_s: float                   # offset from the start of the stream
 
 
+def ygxm_path(points: int) -> dict[str, Any]:
+    """The Y-G-X-M path with ``points`` points (3 segments)."""
+    per = (points - 1) // 3
+    return dict(YGXM, points_per_segment=per)
+
+
+# The serving workload at the sizes it is specified with: 216-8000 atoms
+# (cubic sides 6-20), 16-256 k points per request (drawn from a 301-point
+# Y-G-X-M path), windows of 20-200 Gamma states.
+STREAM_FULL = {"sides": tuple(range(6, 21)), "kpoints": (16, 256), "states": (20, 200),
+               "path_points": 301}
+
+
 def serving_stream(n_requests: int = 12, *, seed: int = 20261203, rate_per_s: float = 2.0,
                    sides: tuple[int, ...] = (6, 7, 8, 9, 10),
-                   kpoints: tuple[int, int] = (4, 16), states: tuple[int, int] = (20, 60)
-                   ) -> list[ServingRequestSpec]:
+                   kpoints: tuple[int, int] = (4, 16), states: tuple[int, int] = (20, 60),
+                   path_points: int = 121) -> list[ServingRequestSpec]:
     """A seeded stream of band requests for the serving benchmark: cubic
     bundles of side**3 atoms (216-1000 with the default sides) with 13
     (Ti-like) or 5 (C-like) orbitals per atom, k points drawn from the
-    121-point Y-G-X-M path, windows holding ``states`` Gamma states, and
-    Poisson arrivals at ``rate_per_s``.  Bundles repeat across requests
-    (same side, orbitals and seed), as a service sees repeated systems."""
+    ``path_points``-point Y-G-X-M path (``ygxm_path``), windows holding
+    ``states`` Gamma states, and Poisson arrivals at ``rate_per_s``.
+    Bundles repeat across requests (same side, orbitals and seed), as a
+    service sees repeated systems."""
     rng = np.random.default_rng(seed)
     out = []
     t = 0.0
@@ -332,7 +346,7 @@ def serving_stream(n_requests: int = 12, *, seed: int = 20261203, rate_per_s: fl
         spec = replace(_cubic(f"serve-{side}-{orbitals}", side, 2.4, 7.0),
                        orbitals_per_atom=orbitals, seed=1000 + side * 17 + orbitals)
         nk = int(rng.integers(kpoints[0], kpoints[1] + 1))
-        ks = tuple(int(v) for v in np.sort(rng.choice(121, size=nk, replace=False)))
+        ks = tuple(int(v) for v in np.sort(rng.choice(path_points, size=nk, replace=False)))
         st = int(rng.integers(states[0], states[1] + 1))
         out.append(ServingRequestSpec(spec, ks, st, t))
         t += float(rng.exponential(1.0 / rate_per_s))

@@ -75,6 +75,10 @@ def parse() -> argparse.Namespace:
                     help="CTAs per SM of the tensor-core solve update (0 = default)")
     ap.add_argument("--tensor-core-solves", type=int, default=-1,
                     help="1/0: split-BF16 tensor-core solve updates on/off (-1 = engine default)")
+    ap.add_argument("--stream", choices=("reduced", "full"), default="reduced",
+                    help="c4 serving stream sizes")
+    ap.add_argument("--requests", type=int, default=0,
+                    help="c4: requests of the seeded stream (0: 12 reduced, 6 full)")
     ap.add_argument("--fp64-check", type=int, default=2,
                     help="k points refined in FP64 (fp64check) when dense FP64 eigh does not fit")
     ap.add_argument("--accuracy-sweep", default="",
@@ -314,11 +318,60 @@ def reference_arm(args) -> None:
     print(json.dumps(out), flush=True)
 
 
+def serving_window(bundle, states: int, dev) -> tuple[float, float]:
+    """Window around the median Gamma eigenvalue holding ``states`` states.
+    Up to n = 16000 from the FP64 dense Gamma spectrum on the device; above,
+    scaled from the dense spectrum of the 8x8x8 bundle with the same
+    orbitals and generator (same on-site and hopping statistics): the
+    density of states per orbital around its median, times n."""
+    import torch
+
+    from aospectrum_b200 import synth
+
+    def spectrum(b):
+        h, s = synth.dense_gamma(b)
+        hd = torch.from_numpy(h).to(dev)
+        sd = torch.from_numpy(s).to(dev)
+        lc = torch.linalg.cholesky(sd)
+        li = torch.linalg.solve_triangular(lc, torch.eye(h.shape[0], dtype=hd.dtype, device=dev),
+                                           upper=False)
+        e = np.sort(torch.linalg.eigvalsh(li @ hd @ li.T).cpu().numpy())
+        del hd, sd, lc, li
+        torch.cuda.empty_cache()
+        return e
+
+    n = bundle.n_orbitals
+    if n <= 16000:
+        e = spectrum(bundle)
+        c = float(np.median(e))
+        dist = np.sort(np.abs(e - c))
+        half = 0.5 * (dist[states - 1] + dist[states])
+        return c - half, c + half
+    spec = bundle.provenance["spec"]
+    small = synth.generate_bundle(synth.SyntheticSpec(**{
+        **{k: tuple(v) if isinstance(v, list) else v for k, v in spec.items()},
+        "name": spec["name"] + "-dos", "grid": (8, 8, 8), "cell": (19.2, 19.2, 19.2)}))
+    e = spectrum(small)
+    c = float(np.median(e))
+    dist = np.sort(np.abs(e - c))
+    probe = max(20, states * small.n_orbitals // n)
+    width = float(dist[probe])           # half width holding `probe` states of the small bundle
+    per_orbital = probe / (2.0 * width * small.n_orbitals)
+    half = states / (2.0 * per_orbital * n)
+    return c - half, c + half
+
+
 def serving_arm(args) -> None:
-    """Serving stream (c4, reduced sizes): seeded Poisson arrivals of band
-    requests over 216-1000-atom bundles through BandServer (continuous
-    batching, mixed precision), against serial plain solves of the same
-    requests on the same GPU."""
+    """Serving stream (c4): seeded Poisson arrivals of band requests through
+    BandServer (continuous batching, mixed precision) against serial plain
+    solves of the same requests on the same GPU.  ``--stream reduced``:
+    216-1000-atom bundles, 4-16 k points, 20-60 states, 12 requests;
+    ``--stream full``: the sizes the workload is specified with (216-8000
+    atoms, 16-256 k points, 20-200 states; ``--requests`` of the seeded
+    stream, 6 by default).  The serial plain baseline is measured: with
+    ``full`` each request's plain time is its k count times one measured
+    plain k point of its bundle and window (every request runs one), and the
+    serial latencies replay the arrivals with those durations."""
     import torch
 
     from aospectrum_b200 import synth
@@ -330,9 +383,11 @@ def serving_arm(args) -> None:
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    stream = synth.serving_stream()
-    kpts = kpath_from_dict(synth.YGXM).fractional_points
-    settings = CissSettings()
+    full = args.stream == "full"
+    preset = synth.STREAM_FULL if full else {}
+    n_req = args.requests or (6 if full else 12)
+    stream = synth.serving_stream(n_req, **preset)
+    kpts = kpath_from_dict(synth.ygxm_path(preset.get("path_points", 121))).fractional_points
     bundles, windows = {}, {}
     for r in stream:
         key = r.spec.name
@@ -340,70 +395,97 @@ def serving_arm(args) -> None:
             bundles[key] = synth.generate_bundle(r.spec)
         wk = (key, r.states)
         if wk not in windows:
-            h, s = synth.dense_gamma(bundles[key])
-            hd = torch.from_numpy(h).to(dev)
-            sd = torch.from_numpy(s).to(dev)
-            lc = torch.linalg.cholesky(sd)
-            li = torch.linalg.solve_triangular(lc, torch.eye(h.shape[0], dtype=hd.dtype,
-                                                             device=dev), upper=False)
-            e = np.sort(torch.linalg.eigvalsh(li @ hd @ li.T).cpu().numpy())
-            c = float(np.median(e))
-            dist = np.sort(np.abs(e - c))
-            half = 0.5 * (dist[r.states - 1] + dist[r.states])
-            windows[wk] = (c - half, c + half)
-            del hd, sd, lc, li
-            torch.cuda.empty_cache()
+            windows[wk] = serving_window(bundles[key], r.states, dev)
+
+    def settings_for(states: int) -> CissSettings:
+        # search dimension L*M comfortably above the window's state count
+        return CissSettings(block_size=32 if states <= 90 else 64)
+
     reqs = [BandRequest(bundles[r.spec.name], [kpts[i] for i in r.kpoint_indices],
-                        EnergyInterval(*windows[(r.spec.name, r.states)]), settings,
-                        f"r{i}") for i, r in enumerate(stream)]
+                        EnergyInterval(*windows[(r.spec.name, r.states)]),
+                        settings_for(r.states), f"r{i}") for i, r in enumerate(stream)]
     total_k = sum(len(r.kpoint_indices) for r in stream)
-    # continuous batching: submit at the seeded arrival times
-    with BandServer(device=dev, slots=4, engine_settings=EngineSettings(precision="mixed")) as srv:
-        t0 = time.perf_counter()
-        futs = []
-        for r, q in zip(stream, reqs):
-            delay = r.arrival_s - (time.perf_counter() - t0)
-            if delay > 0:
-                time.sleep(delay)
-            futs.append(srv.submit(q))
-        responses = [f.result() for f in futs]
-        span = time.perf_counter() - t0
-        stats = srv.stats()
-    # serial plain baseline: one request at a time, plain complex64 batched
-    # engine, arrivals replayed on the same clock
-    serial_lat = []
+    with ClockSampler(0) as clocks:
+        with BandServer(device=dev, slots=4,
+                        engine_settings=EngineSettings(precision="mixed")) as srv:
+            t0 = time.perf_counter()
+            futs = []
+            for r, q in zip(stream, reqs):
+                delay = r.arrival_s - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                futs.append(srv.submit(q))
+            responses = [f.result() for f in futs]
+            span = time.perf_counter() - t0
+            stats = srv.stats()
+    # serial plain baseline: one request at a time, plain complex64 engine
+    serial_lat, durations, measured = [], [], {}
     engines = {}
     t0 = time.perf_counter()
     for r, q in zip(stream, reqs):
-        now = time.perf_counter() - t0
-        if now < r.arrival_s:
-            time.sleep(r.arrival_s - now)
-        key = r.spec.name
-        if key not in engines:
-            engines[key] = BandEngine(q.bundle, settings, EngineSettings(precision="plain"),
-                                      device=dev)
-        engines[key].solve_kpoints(q.kpoints, q.interval)
-        torch.cuda.synchronize(dev)
-        serial_lat.append(time.perf_counter() - t0 - r.arrival_s)
-    serial_span = time.perf_counter() - t0
+        key = (r.spec.name, r.states)
+        ekey = (r.spec.name, q.settings.block_size)   # the probe block is per engine
+        if ekey not in engines:
+            for e in engines.values():
+                e.close()
+            engines = {ekey: BandEngine(q.bundle, q.settings, EngineSettings(precision="plain"),
+                                        device=dev)}
+        eng = engines[ekey]
+        if full:
+            if key not in measured:
+                eng.solve_kpoints(q.kpoints[:1], q.interval)        # warm
+                torch.cuda.synchronize(dev)
+                t1 = time.perf_counter()
+                eng.solve_kpoints(q.kpoints[1:2] or q.kpoints[:1], q.interval)
+                torch.cuda.synchronize(dev)
+                measured[key] = time.perf_counter() - t1
+            durations.append(measured[key] * len(q.kpoints))
+        else:
+            now = time.perf_counter() - t0
+            if now < r.arrival_s:
+                time.sleep(r.arrival_s - now)
+            t1 = time.perf_counter()
+            eng.solve_kpoints(q.kpoints, q.interval)
+            torch.cuda.synchronize(dev)
+            durations.append(time.perf_counter() - t1)
+            serial_lat.append(time.perf_counter() - t0 - r.arrival_s)
     for e in engines.values():
         e.close()
+    if full:
+        clock = 0.0
+        for r, d in zip(stream, durations):
+            clock = max(clock, r.arrival_s) + d
+            serial_lat.append(clock - r.arrival_s)
+        serial_span = clock
+    else:
+        serial_span = time.perf_counter() - t0
     lat = [x.latency_seconds for x in responses]
+    sizes = [{"atoms": int(np.prod(r.spec.grid)), "orbitals": r.spec.orbitals_per_atom,
+              "n": r.spec.n_orbitals, "kpoints": len(r.kpoint_indices), "states": r.states,
+              "block_size": settings_for(r.states).block_size,
+              "arrival_s": round(r.arrival_s, 3)} for r in stream]
+    desc = ("c4 serving stream at the specified sizes: first %d requests of the seeded stream "
+            "(216-8000-atom cubic bundles, 5 or 13 orbitals, 16-256 k points from a 301-point "
+            "Y-G-X-M path, windows of 20-200 Gamma states), Poisson arrivals at 2/s" % n_req
+            if full else
+            "c4 serving stream, reduced sizes: 12 requests, 216-1000-atom cubic bundles, 5 or "
+            "13 orbitals, 4-16 k points, windows of 20-60 Gamma states, Poisson arrivals at 2/s")
     out = {"metric": "serving k-points/s with p50/p99 latency (continuous batching, 1 B200)",
            "value": total_k / span, "unit": "k-points/s", "n_gpus": 1, "steps": 1, "warmup": 0,
            "ms_per_step": span * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "c64+bf16x3 tensor-core updates, fp64 refinement",
            "data": "synthetic (seeded serving stream)",
-           "config": {"workload": "c4 serving stream, reduced sizes: 12 requests, 216-1000-atom "
-                                  "cubic bundles, 5 or 13 orbitals, 4-16 k points, windows of "
-                                  "20-60 Gamma states, Poisson arrivals at 2/s",
-                      "requests": len(stream), "kpoints": total_k, "slots": 4,
-                      "bundles": sorted({r.spec.name for r in stream})},
+           "config": {"workload": desc, "requests": len(stream), "kpoints": total_k, "slots": 4,
+                      "bundles": sorted({r.spec.name for r in stream}), "sizes": sizes},
            "p50_latency_s": percentile(lat, 50), "p99_latency_s": percentile(lat, 99),
-           "server_stats": stats,
+           "server_stats": stats, "clocks": clocks.summary(),
            "serial_plain": {"kpoints_per_s": total_k / serial_span,
                             "p50_latency_s": percentile(serial_lat, 50),
-                            "p99_latency_s": percentile(serial_lat, 99)},
+                            "p99_latency_s": percentile(serial_lat, 99),
+                            "method": ("each request's duration = its k count x one measured "
+                                       "plain k point of its bundle and window; arrivals "
+                                       "replayed" if full else
+                                       "every request solved, arrivals replayed")},
            "max_residual_ev": max(x.maximum_residual_ev for x in responses)}
     print(json.dumps(out), flush=True)
 
@@ -813,6 +895,8 @@ def main() -> None:
         # end to end through the public engine API with host buffers
         if not args.no_e2e:
             out["e2e"] = e2e_leg(eng, bundle, kset, interval, args)
+        if world == 1:
+            out["ingest"] = ingest_leg(bundle, dev)
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(bundle, [kpts[0]], interval.lower_ev,
                                                interval.upper_ev, w)
@@ -852,6 +936,56 @@ def fp64_window(pair, interval, dev) -> np.ndarray:
     return np.sort(e[(e > interval.lower_ev) & (e < interval.upper_ev)])
 
 
+def ingest_leg(bundle, dev) -> dict:
+    """Bundle ingest on this box: the bundle is written to a
+    temporary directory (untimed), then opened memory-mapped (load_bundle),
+    its CSR pattern and Bloch tables built by the C++ host code
+    (aosb_bloch_create), the block values copied from the memory map into
+    pinned host memory and from there to the device."""
+    import tempfile
+
+    import torch
+
+    from aospectrum_b200.bundle import load_bundle, write_bundle
+    from aospectrum_b200.engine import BlochDevice
+
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        root = Path(tmp) / "bundle"
+        write_bundle(bundle, root)
+        t0 = time.perf_counter()
+        loaded = load_bundle(root)
+        out["open_memmap_s"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        bd = BlochDevice(loaded, dev, upload=False)
+        out["pattern_build_cpp_s"] = time.perf_counter() - t0
+        ops = loaded.operators
+        nbytes = 0
+        t0 = time.perf_counter()
+        pinned = []
+        for arr in (ops.h_values, ops.s_values):
+            a = np.asarray(arr)
+            t = torch.empty(a.shape, dtype=torch.from_numpy(a[:1].copy()).dtype, pin_memory=True)
+            t.numpy()[...] = a
+            pinned.append(t)
+            nbytes += a.nbytes
+        out["memmap_to_pinned_s"] = time.perf_counter() - t0
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        dev_copies = [t.to(dev, non_blocking=True) for t in pinned]
+        torch.cuda.synchronize(dev)
+        out["pinned_to_device_s"] = time.perf_counter() - t0
+        out["value_bytes"] = nbytes
+        out["pinned_to_device_gbs"] = nbytes / out["pinned_to_device_s"] / 1e9
+        t0 = time.perf_counter()
+        bd.upload()
+        torch.cuda.synchronize(dev)
+        out["tables_and_values_upload_s"] = time.perf_counter() - t0
+        bd.close()
+        del dev_copies, pinned, loaded
+    return {k: (round(v, 4) if isinstance(v, float) else v) for k, v in out.items()}
+
+
 def e2e_leg(eng, bundle, kset, interval, args) -> dict:
     """Public-API path with host buffers: every step copies the bundle's
     block values from pinned host memory into the engine and reads the
@@ -860,7 +994,9 @@ def e2e_leg(eng, bundle, kset, interval, args) -> dict:
 
     hv = torch.from_numpy(np.array(bundle.operators.h_values)).pin_memory()
     sv = torch.from_numpy(np.array(bundle.operators.s_values)).pin_memory()
-    steps = max(1, args.steps)
+    # at most 20 steps: on the large workloads the timed region already
+    # covers every k point of the path, and this leg repeats the same work
+    steps = max(1, min(args.steps, 20))
     eng.load_values(hv, sv)
     eng.solve_kpoints(kset(0), interval)
     torch.cuda.synchronize()
