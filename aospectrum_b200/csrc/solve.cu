@@ -19,6 +19,7 @@
 
 #include <cuda_bf16.h>
 
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -28,7 +29,72 @@ int solve_graph(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size
 int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, int op, int np,
                     int nrhs, const aosb_plan* P, const float* factor, float2* work,
                     const float2* ytmp, const unsigned char* ystaged, int32_t* status,
-                    cudaStream_t st, char* err, size_t cap);
+                    cudaStream_t st, char* err, size_t cap, int copy_y);
+
+// 1: the tensor-core sweeps run the next step's diagonal solve on a side
+// stream beside the current step's remaining updates; process-wide.
+std::atomic<int> g_solve_lookahead{0};
+
+// Scratch block of aosb_solve: a status word per pencil (tensor-core
+// updates), the diagonal result Y [np][T][L] complex64 and, for tile 128,
+// Y as BF16 B-operand planes [np][strips][32 KB]; the tensor-core path
+// keeps two of each (the lookahead writes step k+1's while step k's is
+// read).  Each part starts on a 256-byte boundary.
+struct ScratchLayout {
+  int32_t* status = nullptr;
+  float2* y[2] = {nullptr, nullptr};
+  unsigned char* ystaged[2] = {nullptr, nullptr};
+  size_t bytes = 0;
+};
+static ScratchLayout scratch_layout(const aosb_plan* P, int np, int nrhs, void* base) {
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  ScratchLayout l;
+  unsigned char* p = (unsigned char*)base;
+  size_t off = 0;
+  l.status = (int32_t*)(p + off);
+  off = up(off + (size_t)np * sizeof(int32_t));
+  const size_t ybytes = up((size_t)np * P->T * nrhs * sizeof(float2));
+  const int copies = P->T == 128 ? 2 : 1;
+  for (int c = 0; c < copies; ++c) {
+    l.y[c] = (float2*)(p + off);
+    off += ybytes;
+  }
+  if (P->T == 128) {
+    const size_t strips = (size_t)((nrhs + tc::kSolveNS - 1) / tc::kSolveNS);
+    const size_t sb = up((size_t)np * strips * tc::kSolveBBytes);
+    for (int c = 0; c < 2; ++c) {
+      l.ystaged[c] = p + off;
+      off += sb;
+    }
+  }
+  l.bytes = off;
+  return l;
+}
+
+// Side stream of a caller stream for the solve lookahead (created once,
+// non-blocking, kept for the life of the process).
+static int solve_side_stream(cudaStream_t main, cudaStream_t* out, char* err, size_t cap) {
+  static std::mutex mu;
+  static std::vector<std::pair<cudaStream_t, cudaStream_t>> table;
+  int device = 0;
+  cudaGetDevice(&device);
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto& e : table) {
+    if (e.first == main) {
+      int dev2 = -1;
+      if (cudaStreamGetDevice(e.second, &dev2) == cudaSuccess && dev2 == device) {
+        *out = e.second;
+        return 0;
+      }
+    }
+  }
+  cudaStream_t s = nullptr;
+  AOSB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), err, cap);
+  table.emplace_back(main, s);
+  *out = s;
+  return 0;
+}
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -191,37 +257,34 @@ int run_solve(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t
   constexpr int BM = T >= 64 ? 64 : 32;
   const int rowblocks = T / BM;
   float2* W = (float2*)a->work;
-  float2* Y = (float2*)a->scratch;
   const bool tc = T == 128 && (a->flags & AOSB_SOLVE_TENSOR_CORES) != 0;
-  // scratch: Y [np][T][L] complex64 | status [np] int32 | (tensor cores) Y
-  // as BF16 B-operand planes [np][strips][32 KB], 128-byte aligned
-  int32_t* tc_status = (int32_t*)((unsigned char*)a->scratch + (size_t)np * T * L * sizeof(float2));
-  unsigned char* ystaged = nullptr;
-  if (tc) {
-    const size_t off = (size_t)np * T * L * sizeof(float2) + (size_t)np * sizeof(int32_t);
-    ystaged = (unsigned char*)a->scratch + ((off + 127) & ~(size_t)127);
-  }
-  auto diag = [&](int k, int op) {
+  const ScratchLayout sl = scratch_layout(P, np, L, a->scratch);
+  int32_t* tc_status = sl.status;
+  auto diag = [&](int k, int op, int buf, cudaStream_t s) {
     count_launches(1);
     dim3 g(ncs, T / 32, np);
     cudaEvent_t ev[2];
-    const bool timed = timing_begin(st, ev);
+    const bool timed = timing_begin(s, ev);
+    float2* Y = sl.y[buf];
+    unsigned char* ys = tc ? sl.ystaged[buf] : nullptr;
     switch (op) {
-      case kLinv: solve_diag_kernel<T, kLinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
-      case kUinv: solve_diag_kernel<T, kUinv><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
-      case kUinvH: solve_diag_kernel<T, kUinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
-      default: solve_diag_kernel<T, kLinvH><<<g, kThreads, 0, st>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ystaged); break;
+      case kLinv: solve_diag_kernel<T, kLinv><<<g, kThreads, 0, s>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ys); break;
+      case kUinv: solve_diag_kernel<T, kUinv><<<g, kThreads, 0, s>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ys); break;
+      case kUinvH: solve_diag_kernel<T, kUinvH><<<g, kThreads, 0, s>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ys); break;
+      default: solve_diag_kernel<T, kLinvH><<<g, kThreads, 0, s>>>(k, L, P->n_pad, P->d_diag_slot, P->n_slots, a->factor, a->pivots, W, Y, ys); break;
     }
     // algorithmic: one triangular T x T tile times T x L per pencil
     if (timed)
-      timing_end(kTimedSolveDiag, st, ev, 4.0 * T * T * L * np,
+      timing_end(kTimedSolveDiag, s, ev, 4.0 * T * T * L * np,
                  (double)np * (2.0 * T * T * sizeof(float) + 2.0 * T * L * sizeof(float2)));
   };
   if (tc) AOSB_CUDA_TRY(cudaMemsetAsync(tc_status, 0, (size_t)np * sizeof(int32_t), st), err, cap);
   int tc_rc = 0;
-  auto update = [&](int k, const std::vector<int32_t>& off, const int32_t* dtiles,
-                    const int32_t* dslots, int op) {
-    const int n = off[k + 1] - off[k];
+  // update of step k with the list entries [b, e) of off[k] .. off[k + 1]
+  auto update = [&](int k, int64_t b, int64_t e, const int32_t* dtiles, const int32_t* dslots,
+                    int op, int buf, bool copy) {
+    const int n = (int)(e - b);
+    if (tc && n == 0 && !copy) return;
     cudaEvent_t ev[2];
     const bool timed = timing_begin(st, ev);
     // algorithmic: n tiles x (T x T) x (T x L) complex per pencil; factor
@@ -230,41 +293,89 @@ int run_solve(const aosb_plan* P, const aosb_solve_args_v1* a, char* err, size_t
     const double ubytes = (double)n * np * (2.0 * T * T * sizeof(float) + 2.0 * T * L * sizeof(float2));
     if (tc) {
       if (tc_rc == 0)
-        tc_rc = solve_tc_update(k, n, dtiles + off[k], dslots + off[k], op, np, L, P, a->factor,
-                                W, Y, ystaged, tc_status, st, err, cap);
+        tc_rc = solve_tc_update(k, n, dtiles + b, dslots + b, op, np, L, P, a->factor, W,
+                                sl.y[buf], sl.ystaged[buf], tc_status, st, err, cap, copy ? 1 : 0);
       if (timed) timing_end(kTimedSolveUpdate, st, ev, uflops, ubytes);
       return;
     }
     dim3 g((unsigned)(n * rowblocks * ncs + kCopyBlocks), np);
     count_launches(1);
     if (op == kPlain)
-      solve_update_kernel<T, kPlain><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + off[k], dslots + off[k], P->n_slots, a->factor, W, Y);
+      solve_update_kernel<T, kPlain><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + b, dslots + b, P->n_slots, a->factor, W, sl.y[buf]);
     else
-      solve_update_kernel<T, kConjT><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + off[k], dslots + off[k], P->n_slots, a->factor, W, Y);
+      solve_update_kernel<T, kConjT><<<g, kThreads, 0, st>>>(k, n, L, P->n_pad, dtiles + b, dslots + b, P->n_slots, a->factor, W, sl.y[buf]);
     if (timed) timing_end(kTimedSolveUpdate, st, ev, uflops, ubytes);
   };
   const int nb = (int)P->nb;
-  if (!a->adjoint) {
-    for (int k = 0; k < nb; ++k) {
-      diag(k, kLinv);
-      update(k, P->lb_off, P->d_lb_tile, P->d_lb_slot, kPlain);
-    }
-    for (int k = nb - 1; k >= 0; --k) {
-      diag(k, kUinv);
-      update(k, P->ua_off, P->d_ua_tile, P->d_ua_slot, kPlain);
-    }
-  } else {
-    for (int k = 0; k < nb; ++k) {
-      diag(k, kUinvH);
-      // X_i -= U_ki^H w_k for U tiles (k, i), i > k
-      update(k, P->ur_off, P->d_ur_tile, P->d_ur_slot, kConjT);
-    }
-    for (int k = nb - 1; k >= 0; --k) {
-      diag(k, kLinvH);
-      // X_i -= L_ki^H x_k for L tiles (k, i), i < k
-      update(k, P->ll_off, P->d_ll_tile, P->d_ll_slot, kConjT);
+  const bool lookahead = tc && g_solve_lookahead.load() != 0 && nb > 1;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_next = nullptr, ev_diag = nullptr;
+  if (lookahead) {
+    if (int rc = solve_side_stream(st, &side, err, cap)) return rc;
+    AOSB_CUDA_TRY(cudaEventCreateWithFlags(&ev_next, cudaEventDisableTiming), err, cap);
+    if (cudaEventCreateWithFlags(&ev_diag, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventDestroy(ev_next);
+      return set_error(err, cap, AOSB_ERR_CUDA, "cudaEventCreate failed");
     }
   }
+  struct EventGuard {
+    cudaEvent_t a, b;
+    ~EventGuard() {
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } guard{ev_next, ev_diag};
+  // One sweep over the steps in `order`: without lookahead, per step the
+  // diagonal solve and then all updates.  With lookahead, step k first
+  // updates the tile of the next step (the first list entry going forward,
+  // the last going backward), then the next step's diagonal solve runs on
+  // the side stream into the other Y buffer while the rest of step k's
+  // updates (and the copy X_k = Y) run on the caller stream.
+  auto sweep = [&](bool forward, const std::vector<int32_t>& off,
+                   const std::vector<int32_t>& host_tiles, const int32_t* dtiles,
+                   const int32_t* dslots, int dop, int uop) -> int {
+    auto step_at = [&](int i) { return forward ? i : nb - 1 - i; };
+    if (!lookahead) {
+      for (int i = 0; i < nb; ++i) {
+        const int k = step_at(i);
+        diag(k, dop, 0, st);
+        update(k, off[k], off[k + 1], dtiles, dslots, uop, 0, true);
+      }
+      return 0;
+    }
+    diag(step_at(0), dop, 0, st);
+    for (int i = 0; i < nb; ++i) {
+      const int k = step_at(i), buf = i & 1;
+      const int64_t b = off[k], e = off[k + 1];
+      int64_t nb0 = b, nb1 = b, rb = b, re = e;   // next-step entry [nb0, nb1), rest [rb, re)
+      if (i + 1 < nb) {
+        const int kn = step_at(i + 1);
+        if (forward && e > b && host_tiles[b] == kn) { nb1 = b + 1; rb = b + 1; }
+        if (!forward && e > b && host_tiles[e - 1] == kn) { nb0 = e - 1; nb1 = e; re = e - 1; }
+        update(k, nb0, nb1, dtiles, dslots, uop, buf, false);
+        AOSB_CUDA_TRY(cudaEventRecord(ev_next, st), err, cap);
+        AOSB_CUDA_TRY(cudaStreamWaitEvent(side, ev_next, 0), err, cap);
+        diag(kn, dop, buf ^ 1, side);
+        AOSB_CUDA_TRY(cudaEventRecord(ev_diag, side), err, cap);
+        update(k, rb, re, dtiles, dslots, uop, buf, true);
+        AOSB_CUDA_TRY(cudaStreamWaitEvent(st, ev_diag, 0), err, cap);
+      } else {
+        update(k, b, e, dtiles, dslots, uop, buf, true);
+      }
+    }
+    return 0;
+  };
+  int rc = 0;
+  if (!a->adjoint) {
+    rc = sweep(true, P->lb_off, P->lb_tile, P->d_lb_tile, P->d_lb_slot, kLinv, kPlain);
+    if (rc == 0) rc = sweep(false, P->ua_off, P->ua_tile, P->d_ua_tile, P->d_ua_slot, kUinv, kPlain);
+  } else {
+    // forward: X_i -= U_ki^H w_k for U tiles (k, i), i > k; backward:
+    // X_i -= L_ki^H x_k for L tiles (k, i), i < k
+    rc = sweep(true, P->ur_off, P->ur_tile, P->d_ur_tile, P->d_ur_slot, kUinvH, kConjT);
+    if (rc == 0) rc = sweep(false, P->ll_off, P->ll_tile, P->d_ll_tile, P->d_ll_slot, kLinvH, kConjT);
+  }
+  if (rc) return rc;
   if (tc_rc) return tc_rc;
   return launch_check(err, cap, "solve");
 }
@@ -627,14 +738,7 @@ extern "C" {
 
 size_t aosb_solve_scratch_bytes(const aosb_plan_t* P, int32_t np, int32_t nrhs) {
   if (P == nullptr || np <= 0 || nrhs <= 0) return 0;
-  // diagonal results, one status word per pencil for the tensor-core
-  // updates and (tile 128) the diagonal results as BF16 B-operand planes
-  size_t bytes = (size_t)np * (size_t)P->T * (size_t)nrhs * sizeof(float2) + (size_t)np * sizeof(int32_t);
-  if (P->T == 128) {
-    const size_t strips = (size_t)((nrhs + aosb::tc::kSolveNS - 1) / aosb::tc::kSolveNS);
-    bytes = ((bytes + 127) & ~(size_t)127) + (size_t)np * strips * aosb::tc::kSolveBBytes;
-  }
-  return bytes;
+  return aosb::scratch_layout(P, np, nrhs, nullptr).bytes;
 }
 
 int aosb_solve_check(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* err, size_t cap) {
@@ -647,8 +751,7 @@ int aosb_solve_check(const aosb_plan_t* P, const aosb_solve_args_v1* a, char* er
   AOSB_CUDA_TRY(cudaStreamSynchronize(st), err, cap);
   if (P->T != 128 || (a->flags & AOSB_SOLVE_TENSOR_CORES) == 0) return 0;
   std::vector<int32_t> host((size_t)a->n_pencils);
-  const unsigned char* words =
-      (const unsigned char*)a->scratch + (size_t)a->n_pencils * P->T * a->n_rhs * sizeof(float2);
+  const int32_t* words = aosb::scratch_layout(P, a->n_pencils, a->n_rhs, a->scratch).status;
   AOSB_CUDA_TRY(cudaMemcpy(host.data(), words, host.size() * sizeof(int32_t),
                            cudaMemcpyDeviceToHost), err, cap);
   for (size_t i = 0; i < host.size(); ++i)
@@ -784,3 +887,8 @@ int aosb_shifted_residual(int64_t n, int32_t nrhs, int32_t np, const int64_t* in
 }
 
 }  // extern "C"
+
+extern "C" int32_t aosb_solve_set_lookahead(int32_t on) {
+  if (on < 0 || on > 1) return -1;
+  return aosb::g_solve_lookahead.exchange(on);
+}

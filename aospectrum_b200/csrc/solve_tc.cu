@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
     const int32_t* __restrict__ slots, int64_t n_slots, float2* __restrict__ work,
     const float2* __restrict__ ytmp, const unsigned char* __restrict__ ystaged,
     int32_t* __restrict__ status, const __grid_constant__ CUtensorMap fmap,
-    const __grid_constant__ CUtensorMap xmap, int x_tma, long long wl) {
+    const __grid_constant__ CUtensorMap xmap, int x_tma, int copy_y, long long wl) {
   const int strips = (nrhs + kNS - 1) / kNS;
   const int total = n_items * strips * n_pencils;
   const int work_ctas = (int)gridDim.x;
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(kSThreads, CTAS) solve_tc_kernel(
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
     const int row = quarter * 32 + lane;
     const int sw = lane & 7;
-    {
+    if (copy_y) {
       // While the first accumulator fills, the epilogue warps of every CTA
       // copy one slice of the step's diagonal result into X_k (X_k = Y for
       // every pencil; no item of this step touches rows of tile k): the
@@ -482,8 +482,8 @@ template <int OP, int CTAS>
 int solve_tc_launch(int k, int n, const int32_t* dtiles, const int32_t* dslots, int np, int nrhs,
                     const aosb_plan* P, float2* work, const float2* ytmp,
                     const unsigned char* ystaged, int32_t* status, const CUtensorMap& fmap,
-                    const CUtensorMap& xmap, int x_tma, int sms, cudaStream_t st, char* err,
-                    size_t cap) {
+                    const CUtensorMap& xmap, int x_tma, int copy_y, int sms, cudaStream_t st,
+                    char* err, size_t cap) {
   const size_t smem = solve_tc_smem<CTAS>();
   // kernel attributes belong to each device's context: set once per device
   static std::atomic<uint64_t> attr_devices{0};
@@ -503,12 +503,16 @@ int solve_tc_launch(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
   const int strips = (nrhs + kNS - 1) / kNS;
   const int64_t items = (int64_t)n * strips * np;
   const int64_t slots = (int64_t)CTAS * sms;
-  // at least one CTA: a step without tiles still copies Y into X_k
-  const int work_ctas = (int)(items < slots ? (items > 0 ? items : 1) : slots);
+  // at least one CTA when the launch copies Y into X_k: a step without
+  // tiles still does that copy
+  const int work_ctas =
+      (int)(items < slots ? (items > 0 ? items : (copy_y ? 1 : 0)) : slots);
+  if (work_ctas == 0) return 0;
   dim3 g((unsigned)work_ctas);
   solve_tc_kernel<OP, CTAS><<<g, kSThreads, smem, st>>>(k, n, nrhs, np, P->n_pad, dtiles, dslots,
                                                         P->n_slots, work, ytmp, ystaged, status,
-                                                        fmap, xmap, x_tma, tc_wait_limit());
+                                                        fmap, xmap, x_tma, copy_y,
+                                                        tc_wait_limit());
   count_launches(1);
   return 0;
 }
@@ -517,7 +521,8 @@ int solve_tc_launch(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
 int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, int op,
                     int np, int nrhs, const aosb_plan* P, const float* factor, float2* work,
                     const float2* ytmp, const unsigned char* ystaged, int32_t* status,
-                    cudaStream_t st, char* err, size_t cap) {
+                    cudaStream_t st, char* err, size_t cap, int copy_y) {
+  if (n == 0 && !copy_y) return 0;
   // the factor as [rows][128] FP32; plain slabs are {16, 128} boxes,
   // adjoint slabs {128, 16}
   CUtensorMap fmap;
@@ -544,13 +549,13 @@ int solve_tc_update(int k, int n, const int32_t* dtiles, const int32_t* dslots, 
   const bool two = g_solve_ctas.load() == 2;
   if (op == kOpPlain)
     return two ? solve_tc_launch<kOpPlain, 2>(k, n, dtiles, dslots, np, nrhs, P, work, ytmp,
-                                              ystaged, status, fmap, xmap, x_tma, sms, st, err, cap)
+                                              ystaged, status, fmap, xmap, x_tma, copy_y, sms, st, err, cap)
                : solve_tc_launch<kOpPlain, 1>(k, n, dtiles, dslots, np, nrhs, P, work, ytmp,
-                                              ystaged, status, fmap, xmap, x_tma, sms, st, err, cap);
+                                              ystaged, status, fmap, xmap, x_tma, copy_y, sms, st, err, cap);
   return two ? solve_tc_launch<kOpConjT, 2>(k, n, dtiles, dslots, np, nrhs, P, work, ytmp, ystaged,
-                                            status, fmap, xmap, x_tma, sms, st, err, cap)
+                                            status, fmap, xmap, x_tma, copy_y, sms, st, err, cap)
              : solve_tc_launch<kOpConjT, 1>(k, n, dtiles, dslots, np, nrhs, P, work, ytmp, ystaged,
-                                            status, fmap, xmap, x_tma, sms, st, err, cap);
+                                            status, fmap, xmap, x_tma, copy_y, sms, st, err, cap);
 }
 
 }  // namespace aosb

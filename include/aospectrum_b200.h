@@ -394,6 +394,13 @@ int aosb_solve_check(const aosb_plan_t *plan, const aosb_solve_args_v1 *args,
  * outside 0..2).  No counterpart in the reference (cuDSS schedules
  * internally). */
 int32_t aosb_solve_set_ctas_per_sm(int32_t ctas);
+/* 1: the tensor-core sweeps (AOSB_SOLVE_TENSOR_CORES) update the next
+ * step's tile first and run the next diagonal solve on a side stream
+ * beside the rest of the current step's updates (double-buffered diagonal
+ * results; same arithmetic, same results); 0: one diagonal solve and one
+ * update per step in order.  Process-wide; returns the previous setting (-1
+ * for other values).  No counterpart in the reference. */
+int32_t aosb_solve_set_lookahead(int32_t on);
 
 /* work[p][i][:] = complex64(src[p*src_stride + perm[i]*n_rhs + :]), zero for
  * padding rows (src: device complex128 [.][n][n_rhs]). */

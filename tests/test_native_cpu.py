@@ -347,6 +347,9 @@ def test_process_wide_tuning_setters_round_trip():
     assert lib.aosb_solve_set_ctas_per_sm(0) == 1
     assert lib.aosb_solve_set_ctas_per_sm(3) == -1
     assert lib.aosb_solve_set_ctas_per_sm(prev) == 2   # 0 restored the default, 2
+    prev = lib.aosb_solve_set_lookahead(1)
+    assert lib.aosb_solve_set_lookahead(prev) == 1
+    assert lib.aosb_solve_set_lookahead(-1) == -1
     prev = lib.aosb_factor_set_schur_pairs(1)
     assert lib.aosb_factor_set_schur_pairs(prev) == 1
     assert lib.aosb_factor_set_schur_pairs(2) == -1
