@@ -875,9 +875,12 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
           if (int rc = panels(k3, side, reserve)) return rc;
           stage_schur(k3, side);
         }
+        // main launch first: it starts at once either way, and a profiler
+        // that serializes launches then sees the full-grid launch take the
+        // items
+        two_step(ss, false, sms - reserve, st, claim_counter, true);
         two_step(ss, false, reserve, side, claim_counter, false);
         AOSB_CUDA_TRY(cudaEventRecord(ev_panel, side), err, cap);
-        two_step(ss, false, sms - reserve, st, claim_counter, true);
         AOSB_CUDA_TRY(cudaStreamWaitEvent(st, ev_panel, 0), err, cap);
       } else {
         two_step(ss, false, sms);

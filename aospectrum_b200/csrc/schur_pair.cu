@@ -17,8 +17,8 @@
 // accumulator sets still double buffered.
 //
 // Roles (320 threads per CTA):
-//   warp 8 lane 0   producer (both CTAs): one TMA of the CTA's A slab and
-//                   one of its half B slab per 16-wide K slab, into a
+//   warp 8 lane 0   producer (both CTAs): bulk copies of the CTA's A slab
+//                   and of its half of the B slab per 16-wide K slab, into a
 //                   kStages-deep ring, completing on the CTA's own full[]
 //                   barrier.  With a shared item counter the even CTA
 //                   claims each item and hands its index to the odd CTA
@@ -58,7 +58,7 @@ constexpr int kASlabBytes = 4 * kT * kSlabK * 2;    // 16 KB: four planes, 128 r
 constexpr int kBHalfBytes = kASlabBytes / 2;        // 8 KB: four planes, 64 rows
 constexpr int kAPlane = kASlabBytes / 4;            // 4096
 constexpr int kBPlane = kBHalfBytes / 4;            // 2048
-constexpr int kPlanesPerTile = 32;                  // 4 KB plane slabs per staged tile
+constexpr int64_t kTileBytes = kSlabs * kASlabBytes;  // 128 KB per staged tile
 #ifndef AOSB_PAIR_STAGES
 #define AOSB_PAIR_STAGES 6
 #endif
@@ -122,15 +122,6 @@ __device__ __forceinline__ bool mbar_wait_cl(uint64_t* bar, uint32_t parity, lon
   }
   return false;
 }
-__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c2, int c4,
-                                            uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes "
-      "[%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(0), "r"(0), "r"(c2), "r"(0),
-      "r"(c4)
-      : "memory");
-}
 __device__ __forceinline__ void umma2_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
                                            uint32_t accumulate) {
   asm volatile(
@@ -181,10 +172,9 @@ __device__ __forceinline__ Halves halves_of(const int32_t* e, uint32_t rank) {
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_pair_kernel(
     const int32_t* __restrict__ list, int n_pairs, int n_pencils, int64_t n_slots,
-    int64_t buf0_planes, int64_t buf1_planes, int64_t pencil_planes, int32_t* __restrict__ status,
-    int* __restrict__ claim, const __grid_constant__ CUtensorMap tm_a,
-    const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tmap_c,
-    long long wl) {
+    const unsigned char* __restrict__ staging, int64_t buf0_bytes, int64_t buf1_bytes,
+    int64_t pencil_stride, int32_t* __restrict__ status, int* __restrict__ claim,
+    const __grid_constant__ CUtensorMap tmap_c, long long wl) {
   extern __shared__ unsigned char dyn[];
   PairShared& sh = *reinterpret_cast<PairShared*>(
       (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
@@ -265,7 +255,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_p
         bool ok = true;
         for (int s = 0; s < h.n * kSlabs; ++s) {
           const int hh = s / kSlabs, sl = s % kSlabs;
-          const int64_t base = (h.buf[hh] ? buf1_planes : buf0_planes) + (int64_t)p * pencil_planes;
+          const unsigned char* base =
+              staging + (h.buf[hh] ? buf1_bytes : buf0_bytes) + (int64_t)p * pencil_stride;
           if (!mbar_wait_cl(&sh.empty[stage], phase ^ 1, wl)) {
             ok = false;
             break;
@@ -273,10 +264,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_p
           filled |= 1u << stage;
           fill_parity = (fill_parity & ~(1u << stage)) | (phase << stage);
           mbar_expect_tx(&sh.full[stage], kASlabBytes + kBHalfBytes);
-          tma_load_5d(sh.a[stage], &tm_a, 0,
-                      (int)(base + (int64_t)h.a[hh] * kPlanesPerTile + sl * 4), &sh.full[stage]);
-          tma_load_5d(sh.b[stage], &tm_b, (int)rank,
-                      (int)(base + (int64_t)h.b[hh] * kPlanesPerTile + sl * 4), &sh.full[stage]);
+          // the A slab is one contiguous 16 KB block; this CTA's half of
+          // the B slab is, per plane and K half, the 1 KB run of its 64
+          // operand rows
+          bulk_g2s(sh.a[stage], base + (int64_t)h.a[hh] * kTileBytes + sl * kASlabBytes,
+                   kASlabBytes, &sh.full[stage]);
+          const unsigned char* bs = base + (int64_t)h.b[hh] * kTileBytes + sl * kASlabBytes;
+#pragma unroll
+          for (int pl = 0; pl < 4; ++pl)
+#pragma unroll
+            for (int kh = 0; kh < 2; ++kh)
+              bulk_g2s(sh.b[stage] + pl * kBPlane + kh * 1024,
+                       bs + pl * kAPlane + kh * 2048 + rank * 1024, 1024, &sh.full[stage]);
           if (++stage == kStages) { stage = 0; phase ^= 1; }
         }
         if (!ok) {
@@ -536,7 +535,8 @@ int schur_pair_launch(const int32_t* d_list, int64_t n_pairs, int n_pencils, int
   if (n_pairs <= 0) return 0;
   if (n_pairs * (int64_t)n_pencils > INT32_MAX)
     return set_error(err, cap, AOSB_ERR_SIZE, "too many Schur pairs x pencils in one launch");
-  if ((buf0_bytes | buf1_bytes | pencil_stride | staging_bytes) % 4096 != 0)
+  if ((buf0_bytes | buf1_bytes | pencil_stride | staging_bytes) % 4096 != 0 ||
+      ((uintptr_t)staging & 15) != 0)
     return set_error(err, cap, AOSB_ERR_ARGUMENT, "staging offsets must be 4 KB multiples");
   const size_t smem = schur_pair_smem();
   static std::atomic<uint64_t> attr_devices{0};
@@ -551,17 +551,13 @@ int schur_pair_launch(const int32_t* d_list, int64_t n_pairs, int n_pencils, int
                        cudaGetErrorString(e));
     attr_devices.fetch_or(dev_bit);
   }
-  CUtensorMap tm_a, tm_b;
-  const uint64_t planes = (uint64_t)staging_bytes / 4096;
-  if (int rc = encode_staging_5d(staging, planes, false, &tm_a, err, cap)) return rc;
-  if (int rc = encode_staging_5d(staging, planes, true, &tm_b, err, cap)) return rc;
   const int64_t items = n_pairs * n_pencils;
   int clusters = ctas / 2;
   if (clusters < 1) clusters = 1;
   if (claim == nullptr && items < clusters) clusters = (int)items;
   schur_pair_kernel<<<2 * clusters, kThreads, smem, st>>>(
-      d_list, (int)n_pairs, n_pencils, n_slots, buf0_bytes / 4096, buf1_bytes / 4096,
-      pencil_stride / 4096, status, claim, tm_a, tm_b, tmap_c, tc_wait_limit());
+      d_list, (int)n_pairs, n_pencils, n_slots, staging, buf0_bytes, buf1_bytes, pencil_stride,
+      status, claim, tmap_c, tc_wait_limit());
   count_launches(1);
   return 0;
 }

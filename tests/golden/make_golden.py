@@ -201,7 +201,7 @@ def main(reference_root: str) -> None:
     print("golden vectors written to", HERE)
 
 
-def main_c2(reference_root: str, kidx: list[int]) -> None:
+def main_c2(reference_root: str, kidx: list[int], name: str = "c2") -> None:
     import time
 
     sys.path.insert(0, str(Path(reference_root) / "src"))
@@ -277,8 +277,9 @@ def main_c2(reference_root: str, kidx: list[int]) -> None:
                     "seconds": round(time.perf_counter() - t0, 1)})
         manifest["kpoints"][str(i)] = rec
         print("c2 k", i, rec, flush=True)
-    np.savez_compressed(HERE / "c2.npz", **arrays)
-    (HERE / "manifest_c2.json").write_text(json.dumps(manifest, indent=2, sort_keys=True) + "\n")
+    np.savez_compressed(HERE / f"{name}.npz", **arrays)
+    (HERE / f"manifest_{name}.json").write_text(json.dumps(manifest, indent=2, sort_keys=True) +
+                                                "\n")
     shutil.rmtree(tmp)
     print("c2 golden vectors written to", HERE)
 
@@ -289,8 +290,10 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("reference_root", help="root of the reference sources")
     ap.add_argument("--c2", default="", help="record only c2 at these k-path indices")
+    ap.add_argument("--c2-name", default="c2",
+                    help="file stem of the c2 record (c2 -> c2.npz, manifest_c2.json)")
     a = ap.parse_args()
     if a.c2:
-        main_c2(a.reference_root, [int(v) for v in a.c2.split(",")])
+        main_c2(a.reference_root, [int(v) for v in a.c2.split(",")], a.c2_name)
     else:
         main(a.reference_root)
