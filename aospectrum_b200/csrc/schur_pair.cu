@@ -17,19 +17,18 @@
 // accumulator sets still double buffered.
 //
 // Roles (320 threads per CTA):
-//   warp 8 lane 0   producer (both CTAs): bulk copies of the CTA's A slab
-//                   and of its half of the B slab per 16-wide K slab, into a
-//                   kStages-deep ring, completing on the CTA's own full[]
-//                   barrier.  With a shared item counter the even CTA
-//                   claims each item and hands its index to the odd CTA
-//                   (remote store + remote arrive on item_full[]);
-//   warp 9 lane 0   even CTA: MMA issuer -- waits for its own full[] and for
-//                   peer_full[] (the odd CTA's stage is in), issues 12 M = 256
-//                   MMAs per slab, commits the slab's release to empty[] of
-//                   both CTAs and the accumulator to acc_full[] of both
-//                   (multicast commits);
-//                   odd CTA: relay -- waits for its own full[] and arrives
-//                   on the even CTA's peer_full[];
+//   warp 8 lane 0   producer (both CTAs): one tensor-map load of the CTA's
+//                   A slab and one of its half of the B slab per 16-wide K
+//                   slab, into a kStages-deep ring; both CTAs' loads count
+//                   on the even CTA's full[] barrier (.cta_group::2 loads),
+//                   whose expected bytes the even CTA posts for the pair.
+//                   With a shared item counter the even CTA claims each item
+//                   and hands its index to the odd CTA (remote store +
+//                   remote arrive on item_full[]);
+//   warp 9 lane 0   even CTA: MMA issuer -- waits for full[], issues 12
+//                   M = 256 MMAs per slab, commits the slab's release to
+//                   empty[] of both CTAs and the accumulator to acc_full[] of
+//                   both (multicast commits);
 //   warps 0-7       epilogue (both CTAs): TMEM -> 128B-swizzled shared tiles
 //                   -> TMA reduce-add into the CTA's own target (C -= acc);
 //                   every warp of both CTAs releases the accumulator on the
@@ -58,7 +57,7 @@ constexpr int kASlabBytes = 4 * kT * kSlabK * 2;    // 16 KB: four planes, 128 r
 constexpr int kBHalfBytes = kASlabBytes / 2;        // 8 KB: four planes, 64 rows
 constexpr int kAPlane = kASlabBytes / 4;            // 4096
 constexpr int kBPlane = kBHalfBytes / 4;            // 2048
-constexpr int64_t kTileBytes = kSlabs * kASlabBytes;  // 128 KB per staged tile
+constexpr int kPlanesPerTile = 32;                  // 4 KB plane slabs per staged tile
 #ifndef AOSB_PAIR_STAGES
 #define AOSB_PAIR_STAGES 6
 #endif
@@ -72,8 +71,7 @@ struct PairShared {
   alignas(1024) unsigned char a[kStages][kASlabBytes];
   alignas(1024) unsigned char b[kStages][kBHalfBytes];
   alignas(1024) float ep[kEpiWarps][2][32 * 32];
-  uint64_t full[kStages];       // own TMA bytes
-  uint64_t peer_full[kStages];  // even CTA: the odd CTA's stage is in (relay)
+  uint64_t full[kStages];       // even CTA: both CTAs' TMA bytes of a stage
   uint64_t empty[kStages];      // the even CTA's MMA commit, both CTAs
   uint64_t acc_full[2];         // the even CTA's accumulator commit, both CTAs
   uint64_t acc_empty[2];        // even CTA: 16 epilogue warps of both CTAs
@@ -121,6 +119,17 @@ __device__ __forceinline__ bool mbar_wait_cl(uint64_t* bar, uint32_t parity, lon
     if (it > 4096) __nanosleep(64);
   }
   return false;
+}
+// Tensor-map load into this CTA's shared memory whose completion is
+// counted on the barrier at cluster address `bar` (the even CTA's; the
+// .cta_group::2 form lets the odd CTA's loads signal the even CTA).
+__device__ __forceinline__ void tma_load_5d_pair(void* dst, const CUtensorMap* map, int c2, int c4,
+                                                 uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(0), "r"(0), "r"(c2), "r"(0), "r"(c4)
+      : "memory");
 }
 __device__ __forceinline__ void umma2_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
                                            uint32_t accumulate) {
@@ -172,9 +181,10 @@ __device__ __forceinline__ Halves halves_of(const int32_t* e, uint32_t rank) {
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_pair_kernel(
     const int32_t* __restrict__ list, int n_pairs, int n_pencils, int64_t n_slots,
-    const unsigned char* __restrict__ staging, int64_t buf0_bytes, int64_t buf1_bytes,
-    int64_t pencil_stride, int32_t* __restrict__ status, int* __restrict__ claim,
-    const __grid_constant__ CUtensorMap tmap_c, long long wl) {
+    int64_t buf0_planes, int64_t buf1_planes, int64_t pencil_planes, int32_t* __restrict__ status,
+    int* __restrict__ claim, const __grid_constant__ CUtensorMap tm_a,
+    const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tmap_c,
+    long long wl) {
   extern __shared__ unsigned char dyn[];
   PairShared& sh = *reinterpret_cast<PairShared*>(
       (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
@@ -185,7 +195,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_p
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&sh.full[s], 1);
-      mbar_init(&sh.peer_full[s], 1);
       mbar_init(&sh.empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -253,29 +262,24 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_p
         const int p = it / n_pairs;
         const Halves h = halves_of(list + (size_t)(it % n_pairs) * 8, rank);
         bool ok = true;
+        const uint32_t full0 = map_to(&sh.full[0], 0);
         for (int s = 0; s < h.n * kSlabs; ++s) {
           const int hh = s / kSlabs, sl = s % kSlabs;
-          const unsigned char* base =
-              staging + (h.buf[hh] ? buf1_bytes : buf0_bytes) + (int64_t)p * pencil_stride;
+          const int64_t base = (h.buf[hh] ? buf1_planes : buf0_planes) + (int64_t)p * pencil_planes;
           if (!mbar_wait_cl(&sh.empty[stage], phase ^ 1, wl)) {
             ok = false;
             break;
           }
           filled |= 1u << stage;
           fill_parity = (fill_parity & ~(1u << stage)) | (phase << stage);
-          mbar_expect_tx(&sh.full[stage], kASlabBytes + kBHalfBytes);
-          // the A slab is one contiguous 16 KB block; this CTA's half of
-          // the B slab is, per plane and K half, the 1 KB run of its 64
-          // operand rows
-          bulk_g2s(sh.a[stage], base + (int64_t)h.a[hh] * kTileBytes + sl * kASlabBytes,
-                   kASlabBytes, &sh.full[stage]);
-          const unsigned char* bs = base + (int64_t)h.b[hh] * kTileBytes + sl * kASlabBytes;
-#pragma unroll
-          for (int pl = 0; pl < 4; ++pl)
-#pragma unroll
-            for (int kh = 0; kh < 2; ++kh)
-              bulk_g2s(sh.b[stage] + pl * kBPlane + kh * 1024,
-                       bs + pl * kAPlane + kh * 2048 + rank * 1024, 1024, &sh.full[stage]);
+          // the even CTA's full[] counts both CTAs' bytes; the odd CTA's
+          // loads signal it directly
+          if (rank == 0) mbar_expect_tx(&sh.full[stage], 2 * (kASlabBytes + kBHalfBytes));
+          const uint32_t bar = full0 + (uint32_t)(stage * sizeof(uint64_t));
+          tma_load_5d_pair(sh.a[stage], &tm_a, 0,
+                           (int)(base + (int64_t)h.a[hh] * kPlanesPerTile + sl * 4), bar);
+          tma_load_5d_pair(sh.b[stage], &tm_b, (int)rank,
+                           (int)(base + (int64_t)h.b[hh] * kPlanesPerTile + sl * 4), bar);
           if (++stage == kStages) { stage = 0; phase ^= 1; }
         }
         if (!ok) {
@@ -303,7 +307,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_p
         }
         bool first_waited = false;
         if (claim != nullptr) {
-          if (!mbar_wait(&sh.full[stage], phase, wl)) {
+          if (!mbar_wait_cl(&sh.full[stage], phase, wl)) {
             sh.failed = 1;
             atomicCAS(&status[0], 0, (int)AOSB_ERR_TIMEOUT);
             break;
@@ -321,11 +325,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_p
         const uint32_t re = tmem + (uint32_t)acc * 256, im = re + kT;
         bool ok = true;
         for (int s = 0; s < h.n * kSlabs; ++s) {
-          if (!(s == 0 && first_waited) && !mbar_wait(&sh.full[stage], phase, wl)) {
-            ok = false;
-            break;
-          }
-          if (!mbar_wait_cl(&sh.peer_full[stage], phase, wl)) {
+          if (!(s == 0 && first_waited) && !mbar_wait_cl(&sh.full[stage], phase, wl)) {
             ok = false;
             break;
           }
@@ -361,41 +361,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_p
         }
         umma2_commit_both(&sh.acc_full[acc]);
         if (++acc == 2) { acc = 0; acc_phase ^= 1; }
-      }
-    } else if (lane == 0) {
-      // ------------------------------------------------- relay (odd CTA)
-      const uint32_t peer_full0 = map_to(&sh.peer_full[0], 0);
-      int stage = 0;
-      uint32_t phase = 0;
-      for (int j = 0; !sh.failed; ++j) {
-        int it = cluster + j * n_clusters;
-        if (claim != nullptr) {
-          const int r = j % kRing;
-          if (!mbar_wait_cl(&sh.item_full[r], (uint32_t)((j / kRing) & 1), wl)) {
-            sh.failed = 1;
-            atomicCAS(&status[0], 0, (int)AOSB_ERR_TIMEOUT);
-            break;
-          }
-          it = *reinterpret_cast<volatile int*>(&sh.items[r]);
-          if (it < 0) break;
-        } else if (it >= total) {
-          break;
-        }
-        const Halves h = halves_of(list + (size_t)(it % n_pairs) * 8, 1);
-        bool ok = true;
-        for (int s = 0; s < h.n * kSlabs; ++s) {
-          if (!mbar_wait(&sh.full[stage], phase, wl)) {
-            ok = false;
-            break;
-          }
-          remote_arrive(peer_full0 + (uint32_t)(stage * sizeof(uint64_t)));
-          if (++stage == kStages) { stage = 0; phase ^= 1; }
-        }
-        if (!ok) {
-          sh.failed = 1;
-          atomicCAS(&status[it / n_pairs], 0, (int)AOSB_ERR_TIMEOUT);
-          break;
-        }
       }
     }
   } else {
@@ -497,16 +462,21 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_p
     if (lane == 0) bulk_wait_all();
     __syncwarp();
   }
-  // Every role has left its loop.  After a failure the producer waits
-  // (bounded) until each stage it filled has its bytes and the even CTA's
-  // MMA issuer until its MMAs are done; then both CTAs meet before TMEM is
-  // freed (the even CTA's MMAs write the odd CTA's TMEM, and the relay and
-  // epilogue arrive on the even CTA's barriers).
+  // Every role has left its loop.  After a failure the even CTA's producer
+  // waits (bounded) until each stage it filled has both CTAs' bytes, and its
+  // MMA issuer until its MMAs are done.  The odd CTA cannot observe its own
+  // loads (they count on the even CTA's barrier); after a failure it pauses
+  // (bounded, ~0.2 ms) so that any load of a stage the even CTA never
+  // accounted lands first.  Then both CTAs meet before TMEM is freed (the
+  // even CTA's MMAs write the odd CTA's TMEM and the odd CTA's loads and
+  // epilogue signal the even CTA's barriers).
   __syncthreads();
   if (sh.failed) {
-    if (warp == kEpiWarps && lane == 0)
+    if (warp == kEpiWarps && lane == 0 && rank == 0)
       for (int s = 0; s < kStages; ++s)
-        if (filled & (1u << s)) mbar_wait(&sh.full[s], (fill_parity >> s) & 1u);
+        if (filled & (1u << s)) mbar_wait_cl(&sh.full[s], (fill_parity >> s) & 1u, kTcWaitLimit);
+    if (warp == kEpiWarps && lane == 0 && rank == 1 && filled)
+      for (int i = 0; i < 200; ++i) __nanosleep(1000);
     if (warp == kEpiWarps + 1 && lane == 0 && rank == 0 && issued) {
       umma2_commit_local(&sh.drain);
       mbar_wait(&sh.drain, 0);
@@ -535,8 +505,7 @@ int schur_pair_launch(const int32_t* d_list, int64_t n_pairs, int n_pencils, int
   if (n_pairs <= 0) return 0;
   if (n_pairs * (int64_t)n_pencils > INT32_MAX)
     return set_error(err, cap, AOSB_ERR_SIZE, "too many Schur pairs x pencils in one launch");
-  if ((buf0_bytes | buf1_bytes | pencil_stride | staging_bytes) % 4096 != 0 ||
-      ((uintptr_t)staging & 15) != 0)
+  if ((buf0_bytes | buf1_bytes | pencil_stride | staging_bytes) % 4096 != 0)
     return set_error(err, cap, AOSB_ERR_ARGUMENT, "staging offsets must be 4 KB multiples");
   const size_t smem = schur_pair_smem();
   static std::atomic<uint64_t> attr_devices{0};
@@ -551,13 +520,17 @@ int schur_pair_launch(const int32_t* d_list, int64_t n_pairs, int n_pencils, int
                        cudaGetErrorString(e));
     attr_devices.fetch_or(dev_bit);
   }
+  CUtensorMap tm_a, tm_b;
+  const uint64_t planes = (uint64_t)staging_bytes / 4096;
+  if (int rc = encode_staging_5d(staging, planes, false, &tm_a, err, cap)) return rc;
+  if (int rc = encode_staging_5d(staging, planes, true, &tm_b, err, cap)) return rc;
   const int64_t items = n_pairs * n_pencils;
   int clusters = ctas / 2;
   if (clusters < 1) clusters = 1;
   if (claim == nullptr && items < clusters) clusters = (int)items;
   schur_pair_kernel<<<2 * clusters, kThreads, smem, st>>>(
-      d_list, (int)n_pairs, n_pencils, n_slots, staging, buf0_bytes, buf1_bytes, pencil_stride,
-      status, claim, tmap_c, tc_wait_limit());
+      d_list, (int)n_pairs, n_pencils, n_slots, buf0_bytes / 4096, buf1_bytes / 4096,
+      pencil_stride / 4096, status, claim, tm_a, tm_b, tmap_c, tc_wait_limit());
   count_launches(1);
   return 0;
 }

@@ -13,6 +13,13 @@ namespace aosb {
 int encode_f32_2d(void* base, uint64_t inner, uint64_t rows, uint32_t box_x, uint32_t box_y,
                   bool swizzle128, CUtensorMap* map, char* err, size_t cap);
 
+// BF16 view of the split-BF16 staging buffer for the two-CTA Schur update:
+// [plane_slabs][2 K halves][2 operand-row halves][8 rows][64 elements]; a
+// box is one 16 KB A slab (four planes, both row halves) or, with half_b,
+// one 8 KB half of a B slab (four planes, one row half) (tma_map.cu).
+int encode_staging_5d(void* base, uint64_t plane_slabs, bool half_b, CUtensorMap* map, char* err,
+                      size_t cap);
+
 namespace tc {
 
 // Polls (with backoff) of one mbarrier wait before it gives up: the default
