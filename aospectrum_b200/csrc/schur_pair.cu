@@ -338,18 +338,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) schur_p
             A[pl] = umma_desc(sa + pl * kAPlane, alb, sbo);
             Bv[pl] = umma_desc(sb + pl * kBPlane, blb, sbo);
           }
+          // the two accumulators alternate, and MMAs that read the same A
+          // plane follow each other
           const uint32_t first = s == 0 ? 0u : 1u;
           umma2_bf16(re, A[0], Bv[0], idesc_pos, first);
-          umma2_bf16(re, A[0], Bv[1], idesc_pos, 1);
-          umma2_bf16(re, A[1], Bv[0], idesc_pos, 1);
-          umma2_bf16(re, A[2], Bv[2], idesc_neg, 1);
-          umma2_bf16(re, A[2], Bv[3], idesc_neg, 1);
-          umma2_bf16(re, A[3], Bv[2], idesc_neg, 1);
           umma2_bf16(im, A[0], Bv[2], idesc_pos, first);
+          umma2_bf16(re, A[0], Bv[1], idesc_pos, 1);
           umma2_bf16(im, A[0], Bv[3], idesc_pos, 1);
+          umma2_bf16(re, A[1], Bv[0], idesc_pos, 1);
           umma2_bf16(im, A[1], Bv[2], idesc_pos, 1);
+          umma2_bf16(re, A[2], Bv[2], idesc_neg, 1);
           umma2_bf16(im, A[2], Bv[0], idesc_pos, 1);
+          umma2_bf16(re, A[2], Bv[3], idesc_neg, 1);
           umma2_bf16(im, A[2], Bv[1], idesc_pos, 1);
+          umma2_bf16(re, A[3], Bv[2], idesc_neg, 1);
           umma2_bf16(im, A[3], Bv[0], idesc_pos, 1);
           umma2_commit_both(&sh.empty[stage]);
           if (++stage == kStages) { stage = 0; phase ^= 1; }
