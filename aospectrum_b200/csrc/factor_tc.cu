@@ -203,9 +203,6 @@ constexpr int kEpiWarps = 8;
 constexpr int kPThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemColsP = 512;
 constexpr int kItemRing = 8;  // > items the producer can run ahead of the epilogue (~4)
-constexpr uint32_t kAccCols = 256;          // one accumulator set: re [0,128), im [128,256)
-constexpr uint32_t kATmemStageCols = 32;    // four BF16 A planes, 8 columns each
-static_assert(kAccCols + kStagesP * kATmemStageCols <= kTmemColsP, "TMEM A ring");
 
 struct PShared {
   alignas(1024) unsigned char a[kStagesP][kOperandSlabBytes];
@@ -324,17 +321,11 @@ __device__ __forceinline__ int item_target(const ItemMap& m, int pair) {
   return m.tslot[a * m.nU + b];
 }
 
-// kATmem: each slab's four A planes are copied into tensor memory
-// (tcgen05.cp, one ring slot per stage at columns 256 + 32 * stage) and the
-// MMAs read only B from shared memory; one accumulator set (columns
-// 0-255), released by the epilogue as soon as its TMEM loads are done.
-template <bool kATmem>
 __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     const ItemMap map, int n_pencils, int64_t n_slots, const unsigned char* __restrict__ staging,
     const unsigned char* __restrict__ staging1, int64_t staging_pencil_stride,
     int32_t* __restrict__ status, int* __restrict__ claim,
     const __grid_constant__ CUtensorMap tmap_c, long long wl) {
-  constexpr int kAccSets = kATmem ? 1 : 2;
   const int n_pairs = map.n_pairs;
   extern __shared__ unsigned char dyn[];
   PShared& sh = *reinterpret_cast<PShared*>(
@@ -469,39 +460,18 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
             Bv[pl] = umma_desc(sb + pl * kPlaneSlabBytes, lbo, sbo);
           }
           const uint32_t first = s == 0 ? 0u : 1u;
-          if constexpr (kATmem) {
-            // A planes of this stage into its TMEM slot; the slot is
-            // rewritten only after empty[stage] completed, i.e. after the
-            // MMAs below have read it
-            const uint32_t at = tmem + kAccCols + (uint32_t)stage * kATmemStageCols;
-#pragma unroll
-            for (int pl = 0; pl < 4; ++pl) tmem_cp_128x256b(at + pl * 8, A[pl]);
-            umma_bf16_ts(re, at + 0, Bv[0], id_pos, first);
-            umma_bf16_ts(re, at + 0, Bv[1], id_pos, 1);
-            umma_bf16_ts(re, at + 8, Bv[0], id_pos, 1);
-            umma_bf16_ts(re, at + 16, Bv[2], id_neg, 1);
-            umma_bf16_ts(re, at + 16, Bv[3], id_neg, 1);
-            umma_bf16_ts(re, at + 24, Bv[2], id_neg, 1);
-            umma_bf16_ts(im, at + 0, Bv[2], id_pos, first);
-            umma_bf16_ts(im, at + 0, Bv[3], id_pos, 1);
-            umma_bf16_ts(im, at + 8, Bv[2], id_pos, 1);
-            umma_bf16_ts(im, at + 16, Bv[0], id_pos, 1);
-            umma_bf16_ts(im, at + 16, Bv[1], id_pos, 1);
-            umma_bf16_ts(im, at + 24, Bv[0], id_pos, 1);
-          } else {
-            umma_bf16(re, A[0], Bv[0], id_pos, first);
-            umma_bf16(re, A[0], Bv[1], id_pos, 1);
-            umma_bf16(re, A[1], Bv[0], id_pos, 1);
-            umma_bf16(re, A[2], Bv[2], id_neg, 1);
-            umma_bf16(re, A[2], Bv[3], id_neg, 1);
-            umma_bf16(re, A[3], Bv[2], id_neg, 1);
-            umma_bf16(im, A[0], Bv[2], id_pos, first);
-            umma_bf16(im, A[0], Bv[3], id_pos, 1);
-            umma_bf16(im, A[1], Bv[2], id_pos, 1);
-            umma_bf16(im, A[2], Bv[0], id_pos, 1);
-            umma_bf16(im, A[2], Bv[1], id_pos, 1);
-            umma_bf16(im, A[3], Bv[0], id_pos, 1);
-          }
+          umma_bf16(re, A[0], Bv[0], id_pos, first);
+          umma_bf16(re, A[0], Bv[1], id_pos, 1);
+          umma_bf16(re, A[1], Bv[0], id_pos, 1);
+          umma_bf16(re, A[2], Bv[2], id_neg, 1);
+          umma_bf16(re, A[2], Bv[3], id_neg, 1);
+          umma_bf16(re, A[3], Bv[2], id_neg, 1);
+          umma_bf16(im, A[0], Bv[2], id_pos, first);
+          umma_bf16(im, A[0], Bv[3], id_pos, 1);
+          umma_bf16(im, A[1], Bv[2], id_pos, 1);
+          umma_bf16(im, A[2], Bv[0], id_pos, 1);
+          umma_bf16(im, A[2], Bv[1], id_pos, 1);
+          umma_bf16(im, A[3], Bv[0], id_pos, 1);
           umma_commit(&sh.empty[stage]);
           if (++stage == kStagesP) { stage = 0; phase ^= 1; }
         }
@@ -511,7 +481,7 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
           break;
         }
         umma_commit(&sh.acc_full[acc]);
-        if (++acc == kAccSets) { acc = 0; acc_phase ^= 1; }
+        if (++acc == 2) { acc = 0; acc_phase ^= 1; }
       }
     }
   } else {
@@ -551,52 +521,6 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
       const int64_t row0 = ((int64_t)p * n_slots + item_target(map, pair)) * (2 * kTcT);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t base = tmem + (uint32_t)acc * 256 + (uint32_t)half * 64 + lane_addr;
-      if constexpr (kATmem) {
-        // one accumulator set: load all of this warp's columns at once and
-        // release them before the shared-memory and TMA work
-        uint32_t v[4][32];   // re block 0, re block 1, im block 0, im block 1
-        tmem_ld32_async(base, v[0]);
-        tmem_ld32_async(base + 32, v[1]);
-        tmem_ld32_async(base + kTcT, v[2]);
-        tmem_ld32_async(base + kTcT + 32, v[3]);
-        tmem_ld_wait();
-#pragma unroll
-        for (int q = 0; q < 4; ++q) tmem_reg_fence(v[q]);
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sh.acc_empty[acc]);
-#pragma unroll
-        for (int bk = 0; bk < 2; ++bk) {
-          if (lane == 0) bulk_wait_read_all();
-          __syncwarp();
-#pragma unroll
-          for (int c = 0; c < 8; ++c) {
-            const int off = lane * 32 + ((c ^ sw) * 4);
-            *reinterpret_cast<float4*>(bre + off) =
-                make_float4(sgn * __uint_as_float(v[bk][4 * c]), sgn * __uint_as_float(v[bk][4 * c + 1]),
-                            sgn * __uint_as_float(v[bk][4 * c + 2]), sgn * __uint_as_float(v[bk][4 * c + 3]));
-            *reinterpret_cast<float4*>(bim + off) = make_float4(
-                sgn * __uint_as_float(v[2 + bk][4 * c]), sgn * __uint_as_float(v[2 + bk][4 * c + 1]),
-                sgn * __uint_as_float(v[2 + bk][4 * c + 2]), sgn * __uint_as_float(v[2 + bk][4 * c + 3]));
-          }
-          fence_proxy_async_smem();
-          __syncwarp();
-          if (lane == 0) {
-            const int x = half * 64 + bk * 32;
-            const int y = (int)(row0 + quarter * 32);
-            if (store) {
-              tma_store_2d(&tmap_c, bre, x, y);
-              tma_store_2d(&tmap_c, bim, x, y + kTcT);
-            } else {
-              tma_reduce_add_2d(&tmap_c, bre, x, y);
-              tma_reduce_add_2d(&tmap_c, bim, x, y + kTcT);
-            }
-            bulk_commit();
-          }
-        }
-        if (++acc == kAccSets) { acc = 0; acc_phase ^= 1; }
-        continue;
-      }
 #pragma unroll
       for (int bk = 0; bk < 2; ++bk) {
         float vr[2][16], vi[2][16];
@@ -636,7 +560,7 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
           bulk_commit();
         }
       }
-      if (++acc == kAccSets) { acc = 0; acc_phase ^= 1; }
+      if (++acc == 2) { acc = 0; acc_phase ^= 1; }
     }
     // the target updates must be complete (not only read) before exit
     if (lane == 0) bulk_wait_all();
@@ -726,10 +650,6 @@ std::atomic<int> g_lookahead_sms{0};
 // process-wide.
 std::atomic<int> g_schur_pairs{0};
 
-// 1: the Schur and panel products read their A operand from tensor memory
-// (schur_tc_kernel<true>); process-wide.
-std::atomic<int> g_schur_tmem_a{0};
-
 // Polls of one mbarrier wait before a tensor-core kernel gives up and
 // records AOSB_ERR_TIMEOUT; process-wide, read at each launch.
 std::atomic<long long> g_tc_wait_limit{tc::kTcWaitLimit};
@@ -751,16 +671,12 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   static std::atomic<uint64_t> attr_devices{0};
   const uint64_t dev_bit = device < 64 ? (uint64_t)1 << device : 0;
   if (dev_bit == 0 || (attr_devices.load() & dev_bit) == 0) {
-    for (auto* f : {schur_tc_kernel<false>, schur_tc_kernel<true>}) {
-      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess)
-        return set_error(err, cap, AOSB_ERR_CUDA, "schur_tc smem attribute: %s",
-                         cudaGetErrorString(e));
-    }
+    cudaError_t e = cudaFuncSetAttribute(schur_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess)
+      return set_error(err, cap, AOSB_ERR_CUDA, "schur_tc smem attribute: %s", cudaGetErrorString(e));
     attr_devices.fetch_or(dev_bit);
   }
-  auto* const schur_kernel =
-      g_schur_tmem_a.load() != 0 ? schur_tc_kernel<true> : schur_tc_kernel<false>;
   // staged tiles per pencil: the step's L and U tiles plus the two
   // diagonal inverses of the panel product
   const int64_t pencil_stride = staged_tiles_per_pencil(P) * (int64_t)kStagedTileBytes;
@@ -819,7 +735,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
         nL, nU, 1, (int)k, lslot, uslot, P->diag_slot[k], P->n_slots, P->n_pad, a->factor,
         a->pivots, stage_buf(k), pencil_stride);
     const ItemMap pm{kMapPanel, nL, nU, nL + nU, 0, 0, nullptr, lslot, uslot, nullptr};
-    schur_kernel<<<grid_for((int64_t)(nL + nU) * np, cap_ctas), kPThreads, smem, s>>>(
+    schur_tc_kernel<<<grid_for((int64_t)(nL + nU) * np, cap_ctas), kPThreads, smem, s>>>(
         pm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c, wl);
     count_launches(2);
     return 0;
@@ -842,7 +758,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     const int nU = P->ur_off[k + 1] - P->ur_off[k];
     const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr,
                      nullptr};
-    schur_kernel<<<grid_for((int64_t)n_pairs * np, cap_ctas), kPThreads, smem, s>>>(
+    schur_tc_kernel<<<grid_for((int64_t)n_pairs * np, cap_ctas), kPThreads, smem, s>>>(
         sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c, wl);
     count_launches(1);
   };
@@ -856,7 +772,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     const bool timed = timing_begin(st, ev);
     const ItemMap sm{kind, nL, nU, n_pairs, a0, b0, P->d_sc_slot + P->sc_off[k], nullptr, nullptr,
                      nullptr};
-    schur_kernel<<<grid_for(items, cap_ctas), kPThreads, smem, st>>>(
+    schur_tc_kernel<<<grid_for(items, cap_ctas), kPThreads, smem, st>>>(
         sm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c, wl);
     count_launches(1);
     if (timed)
@@ -907,7 +823,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
       if (rc != 0 && pair_rc == 0) pair_rc = rc;
     } else {
       const ItemMap lm{kMapList, 0, 0, (int)n, 0, 0, nullptr, nullptr, nullptr, dev + 5 * off[ss]};
-      schur_kernel<<<grid_for(n * np, cap_ctas), kPThreads, smem, s>>>(
+      schur_tc_kernel<<<grid_for(n * np, cap_ctas), kPThreads, smem, s>>>(
           lm, np, P->n_slots, stage_buf(k0), stage_buf(k0 + 1), pencil_stride, a->status, claim,
           tmap_c, wl);
       count_launches(1);
@@ -1023,11 +939,6 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
 }
 
 }  // namespace aosb
-
-extern "C" int32_t aosb_factor_set_schur_tmem_a(int32_t on) {
-  if (on < 0 || on > 1) return -1;
-  return aosb::g_schur_tmem_a.exchange(on);
-}
 
 extern "C" int32_t aosb_factor_set_schur_pairs(int32_t on) {
   if (on < 0 || on > 1) return -1;

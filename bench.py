@@ -71,9 +71,6 @@ def parse() -> argparse.Namespace:
                     help="SMs left to the factorization's lookahead side stream (0 = default)")
     ap.add_argument("--schur-pairs", type=int, default=-1, choices=(-1, 0, 1),
                     help="two-CTA (M = 256) pair Schur updates: 1 on, 0 off, -1 library default")
-    ap.add_argument("--schur-tmem-a", type=int, default=-1, choices=(-1, 0, 1),
-                    help="Schur/panel MMAs with the A operand in tensor memory: 1 on, 0 off, "
-                         "-1 library default")
     ap.add_argument("--solve-lookahead", type=int, default=-1, choices=(-1, 0, 1),
                     help="next diagonal solve on a side stream: 1 on, 0 off, -1 library default")
     ap.add_argument("--solve-ctas", type=int, default=0, choices=(0, 1, 2),
@@ -630,10 +627,6 @@ def main() -> None:
         native.library().aosb_factor_set_schur_pairs(args.schur_pairs)
     if args.solve_lookahead >= 0:
         native.library().aosb_solve_set_lookahead(args.solve_lookahead)
-    if args.schur_tmem_a >= 0:
-        native.library().aosb_factor_set_schur_tmem_a(args.schur_tmem_a)
-    tmem_a_on = native.library().aosb_factor_set_schur_tmem_a(0)
-    native.library().aosb_factor_set_schur_tmem_a(tmem_a_on)
     look_on = native.library().aosb_solve_set_lookahead(0)
     native.library().aosb_solve_set_lookahead(look_on)
     pairs_on = native.library().aosb_factor_set_schur_pairs(0)
@@ -799,7 +792,6 @@ def main() -> None:
                    "tensor_core_solves": bool(eng.engine.tensor_core_solves),
                    "schur_depth": eng.engine.schur_depth,
                    "schur_pairs": bool(pairs_on),
-                   "schur_tmem_a": bool(tmem_a_on),
                    "solve_lookahead": bool(look_on),
                    "lookahead_sms": args.lookahead_sms or "default",
                    "solve_ctas_per_sm": args.solve_ctas or "default",

@@ -333,14 +333,6 @@ int32_t aosb_factor_set_lookahead_sms(int32_t sms);
  * target per CTA.  Process-wide; returns the previous setting (-1 for
  * other values).  No counterpart in the reference. */
 int32_t aosb_factor_set_schur_pairs(int32_t on);
-/* 1: the tensor-core Schur and panel products copy each K slab of their A
- * operand (the L tile) from shared memory into tensor memory (tcgen05.cp)
- * and the MMAs read only B from shared memory, which halves the operand
- * bytes each MMA pulls through the SM's shared-memory port; one TMEM
- * accumulator set per CTA instead of two.  0: both operands from shared
- * memory.  Process-wide; returns the previous setting (-1 for other
- * values).  No counterpart in the reference. */
-int32_t aosb_factor_set_schur_tmem_a(int32_t on);
 /* Polls of one mbarrier wait in the tensor-core kernels (factorization
  * Schur/panel products and solve updates) before the waiting CTA gives up:
  * it records AOSB_ERR_TIMEOUT in the pencil's status word, waits (with the
