@@ -415,13 +415,20 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel_t(
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
+      // The next item's index (a claim from the shared counter, or the
+      // static stride) and its list entry are fetched one item ahead: the
+      // atomic and the dependent list load then overlap the current item's
+      // copies instead of draining the ring at every item boundary.  A
+      // claimed item is always processed by the CTA that claimed it.
+      int cur = claim != nullptr ? atomicAdd(claim, 1) : (int)blockIdx.x;
+      int ia[2], ib[2], bf[2], nh = 0;
+      if (cur < total) nh = item_halves(map, cur % n_pairs, ia, ib, bf);
+      int nxt = claim != nullptr ? atomicAdd(claim, 1) : cur + (int)gridDim.x;
       for (int j = 0; !sh.failed; ++j) {
-        int it = blockIdx.x + j * (int)gridDim.x;
+        int it = cur < total ? cur : -1;
         if (claim != nullptr) {
           // dynamic: the item index reaches the MMA issuer and the epilogue
           // through sh.items, published by this thread's arrive on full[]
-          it = atomicAdd(claim, 1);
-          if (it >= total) it = -1;
           sh.items[j % kItemRing] = it;
           if (it < 0) {
             // stop token: one slab slot whose full[] completes without data
@@ -433,13 +440,14 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel_t(
             mbar_arrive(&sh.full[stage]);
             break;
           }
-        } else if (it >= total) {
+        } else if (it < 0) {
           break;
         }
-        const int p = it / n_pairs, pair = it % n_pairs;
-        int ia[2], ib[2], bf[2];
-        const int nh = item_halves(map, pair, ia, ib, bf);
-        for (int s = 0; s < nh * kSlabs; ++s) {
+        const int p = it / n_pairs;
+        const int nslabs = nh * kSlabs;
+        int na[2] = {0, 0}, nb[2] = {0, 0}, nf[2] = {0, 0}, nnh = 0;
+        for (int s = 0; s < nslabs; ++s) {
+          if (s == 2 && nxt < total) nnh = item_halves(map, nxt % n_pairs, na, nb, nf);
           const int h = s / kSlabs, sl = s % kSlabs;
           const unsigned char* base = (bf[h] ? staging1 : staging) + (size_t)p * staging_pencil_stride;
           const unsigned char* stA = base + (size_t)ia[h] * kTileBytes;
@@ -457,6 +465,15 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel_t(
           bulk_g2s(sh.b[stage], stB + (size_t)sl * kBSlab, kBSlab, &sh.full[stage]);
           if (++stage == kStagesP) { stage = 0; phase ^= 1; }
         }
+        if (sh.failed) break;
+        cur = nxt;
+        nh = nnh;
+        for (int q = 0; q < 2; ++q) {
+          ia[q] = na[q];
+          ib[q] = nb[q];
+          bf[q] = nf[q];
+        }
+        nxt = cur >= total ? total : claim != nullptr ? atomicAdd(claim, 1) : cur + (int)gridDim.x;
       }
     }
   } else if (warp == kEpiWarps + 1) {
