@@ -86,6 +86,9 @@ def parse() -> argparse.Namespace:
                     help="c4: requests of the seeded stream (0: 12 reduced, 6 full)")
     ap.add_argument("--fp64-check", type=int, default=2,
                     help="k points refined in FP64 (fp64check) when dense FP64 eigh does not fit")
+    ap.add_argument("--fp64-check-interval", choices=("solve", "window"), default="solve",
+                    help="interval of the FP64 check: the solve interval (window plus the "
+                         "0.02 eV continuity guards) or the window alone")
     ap.add_argument("--accuracy-sweep", default="",
                     help="k indices ('all', 'a:b:s' or 'i,j,...'): no timing; per k point, "
                          "mixed and plain eigenvalues and residuals against FP64 dense eigh")
@@ -844,9 +847,12 @@ def main() -> None:
         if not dense_ok and args.fp64_check > 0:
             from aospectrum_b200.fp64check import fp64_check
 
+            check_iv = (EnergyInterval(*w.window_ev) if args.fp64_check_interval == "window"
+                        else interval)
             for i in range(min(args.fp64_check, len(kpts))):
                 kpt = kpts[(i * 37) % len(kpts)]
-                c = fp64_check(eng, kpt, interval)
+                c = fp64_check(eng, kpt, check_iv)
+                c["interval_ev"] = [check_iv.lower_ev, check_iv.upper_ev]
                 c["k_index"] = (i * 37) % len(kpts)
                 checks.append(c)
                 errs.append(c["max_eig_error_ev"] if c.get("max_eig_error_ev") is not None
@@ -855,6 +861,11 @@ def main() -> None:
                            "kpoints_checked": len(errs),
                            "max_residual_ev": max(r.maximum_residual_ev for rs in results
                                                   for r in rs),
+                           # k points whose CISS search space (L x M columns) saturated:
+                           # the interval holds more states than it can resolve
+                           "saturated_kpoints": sum(1 for rs in results for r in rs
+                                                    if not r.complete),
+                           "search_dimension": w.block_size * w.moment_size,
                            "oracle": ("FP64 dense generalized eigh (torch, cuSOLVER) of the "
                                       "same H(k), S(k)" if dense_ok else
                                       "FP64 refinement (aospectrum_b200.fp64check): one "
