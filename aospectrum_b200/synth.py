@@ -287,7 +287,9 @@ WORKLOADS: dict[str, Workload] = {
                    notes="1000 atoms, n=13000, 3D periodic, 121 k"),
     "c3": Workload("c3", SPEC_C3, uniform_grid_kpath(8, 8, 4), (-2.5845, -2.5548), 160,
                    block_size=48, notes="4096 atoms, n=53248, 256 k x 32 nodes"),
-    "c5": Workload("c5", SPEC_C5, YGXM, (-2.52, -2.49), 64,
+    # 48 probes: the window (64 states) plus the 0.02 eV continuity guards
+    # holds about 150 states, more than 32 x 4 search columns resolve
+    "c5": Workload("c5", SPEC_C5, YGXM, (-2.52, -2.49), 64, block_size=48,
                    notes="20000 atoms, n=260000, two-layer slab"),
 }
 
