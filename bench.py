@@ -851,7 +851,11 @@ def main() -> None:
                         else interval)
             for i in range(min(args.fp64_check, len(kpts))):
                 kpt = kpts[(i * 37) % len(kpts)]
-                c = fp64_check(eng, kpt, check_iv)
+                try:
+                    c = fp64_check(eng, kpt, check_iv)
+                except Exception as exc:   # the timed result above still gets printed
+                    c = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+                    torch.cuda.empty_cache()
                 c["interval_ev"] = [check_iv.lower_ev, check_iv.upper_ev]
                 c["k_index"] = (i * 37) % len(kpts)
                 checks.append(c)
