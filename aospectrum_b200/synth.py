@@ -285,7 +285,10 @@ WORKLOADS: dict[str, Workload] = {
                    notes="64 atoms, n=832, 2D periodic, 121-point Y-G-X-M"),
     "c2": Workload("c2", SPEC_C2, YGXM, (-2.6188, -2.5204), 100,
                    notes="1000 atoms, n=13000, 3D periodic, 121 k"),
-    "c3": Workload("c3", SPEC_C3, uniform_grid_kpath(8, 8, 4), (-2.5845, -2.5548), 160,
+    # the window holds 87 states at Gamma (the engine's count, FP64 residuals
+    # <= 1.6e-4 eV); with the 0.02 eV guards the solve interval holds about
+    # 200, more than L x M = 192 resolve
+    "c3": Workload("c3", SPEC_C3, uniform_grid_kpath(8, 8, 4), (-2.5845, -2.5548), 87,
                    block_size=48, notes="4096 atoms, n=53248, 256 k x 32 nodes"),
     # 48 probes: the window (64 states) plus the 0.02 eV continuity guards
     # holds about 150 states, more than 32 x 4 search columns resolve
