@@ -59,6 +59,29 @@ def shift_centres(energies: np.ndarray, eta: float) -> list[tuple[float, list[in
     return out
 
 
+def compare_refined(energies: np.ndarray, refined: np.ndarray, residuals: np.ndarray,
+                    engine_residual: float) -> tuple[np.ndarray, float | None, int]:
+    """Which refined pairs count, and the engine's error against them.
+
+    Only converged refined pairs count: the enriched space also yields Ritz
+    values that approximate no eigenpair (their residuals are of the order
+    of the interval width).  Converged: residual at most 1e-3 eV (the
+    reference's warning level) or twice the engine's own largest residual.
+    The engine's values are paired one to one with the converged refined
+    values at the least total distance; returns (converged mask, max
+    distance over the pairs or None, number of pairs)."""
+    conv = np.asarray(residuals) <= max(1e-3, 2.0 * engine_residual)
+    ref_conv = np.asarray(refined)[conv]
+    energies = np.asarray(energies, dtype=np.float64)
+    if ref_conv.size == 0 or energies.size == 0:
+        return conv, None, 0
+    from scipy.optimize import linear_sum_assignment
+
+    dist = np.abs(energies[:, None] - ref_conv[None, :])
+    rows, cols = linear_sum_assignment(dist)
+    return conv, float(dist[rows, cols].max()), int(rows.size)
+
+
 def fp64_check(engine: Any, kpoint: Sequence[float], interval: EnergyInterval, *,
                eta_ev: float | None = None, tol: float = 1e-9, max_sweeps: int = 30) -> dict:
     """Refine the engine's eigenpairs at one k point (see the module text)
@@ -191,21 +214,9 @@ def fp64_check(engine: Any, kpoint: Sequence[float], interval: EnergyInterval, *
     gaps = np.array([np.min(np.abs(np.delete(e2, i) - e2[i])) for i in sel]) if sel.size else \
         np.zeros(0)
     bound = norms ** 2 / np.maximum(gaps, 1e-300)
-    # Only converged refined pairs count: the enriched space also yields Ritz
-    # values that approximate no eigenpair (their residuals are of the order
-    # of the interval width).  Converged: residual at most 1e-3 eV (the
-    # reference's warning level) or twice the engine's own largest residual.
     engine_res = float(res[0].maximum_residual_ev)
-    conv = norms <= max(1e-3, 2.0 * engine_res)
+    conv, err, paired = compare_refined(energies, refined, norms, engine_res)
     ref_conv = refined[conv]
-    err, paired = None, 0
-    if ref_conv.size and energies.size:
-        from scipy.optimize import linear_sum_assignment
-
-        dist = np.abs(energies[:, None] - ref_conv[None, :])
-        rows, cols = linear_sum_assignment(dist)
-        err = float(dist[rows, cols].max())
-        paired = int(rows.size)
     return {"count": m, "refined_count": int(refined.size), "converged_count": int(ref_conv.size),
             "count_diff": int(m - ref_conv.size), "paired": paired,
             "max_eig_error_ev": err,
