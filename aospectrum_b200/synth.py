@@ -290,9 +290,10 @@ WORKLOADS: dict[str, Workload] = {
     # 200, more than L x M = 192 resolve
     "c3": Workload("c3", SPEC_C3, uniform_grid_kpath(8, 8, 4), (-2.5845, -2.5548), 87,
                    block_size=48, notes="4096 atoms, n=53248, 256 k x 32 nodes"),
-    # 48 probes; the window is 0.01 eV wide: a 0.03 eV window held more
-    # than 192 states (the search columns of L = 48, M = 4) at every k point
-    "c5": Workload("c5", SPEC_C5, YGXM, (-2.51, -2.50), 64, block_size=48,
+    # 48 probes; the window is 5 meV wide: 0.03 eV held more than the 192
+    # search columns of L = 48, M = 4 at every k point, 0.01 eV held 118
+    # states at Gamma
+    "c5": Workload("c5", SPEC_C5, YGXM, (-2.5075, -2.5025), 64, block_size=48,
                    notes="20000 atoms, n=260000, two-layer slab"),
 }
 
