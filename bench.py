@@ -74,6 +74,9 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--schur-wide", type=int, default=-1, choices=(-1, 0, 1),
                     help="Schur/panel products as N = 256 MMAs on wide-staged U tiles: 1 on, "
                          "0 off, -1 library default")
+    ap.add_argument("--cuda-graphs", type=int, default=-1, choices=(-1, 0, 1),
+                    help="replay each batch's triangular sweeps from a CUDA graph: 1 on, 0 off, "
+                         "-1 engine default")
     ap.add_argument("--solve-lookahead", type=int, default=-1, choices=(-1, 0, 1),
                     help="next diagonal solve on a side stream: 1 on, 0 off, -1 library default")
     ap.add_argument("--solve-ctas", type=int, default=0, choices=(0, 1, 2),
@@ -656,7 +659,9 @@ def main() -> None:
                                     **({"refinement_steps": args.refinement_steps}
                                        if args.refinement_steps >= 0 else {}),
                                     **({"tensor_core_solves": bool(args.tensor_core_solves)}
-                                       if args.tensor_core_solves >= 0 else {})), device=dev)
+                                       if args.tensor_core_solves >= 0 else {}),
+                                    **({"cuda_graphs": bool(args.cuda_graphs)}
+                                       if args.cuda_graphs >= 0 else {})), device=dev)
     kpts = kp.fractional_points
     tuning = eng.tuning.as_dict() if eng.tuning is not None else None
     if args.kpoints_per_step:
@@ -800,6 +805,7 @@ def main() -> None:
                    "refinement_steps": eng.engine.refinement_steps if args.precision == "mixed"
                    else 0,
                    "tensor_core_solves": bool(eng.engine.tensor_core_solves),
+                   "cuda_graphs": bool(eng.engine.cuda_graphs),
                    "schur_depth": eng.engine.schur_depth,
                    "schur_pairs": bool(pairs_on),
                    "schur_wide": bool(wide_on) and not bool(pairs_on),
