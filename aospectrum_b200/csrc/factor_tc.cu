@@ -19,16 +19,6 @@
 //       Re += Lr_h Ur_h + Lr_h Ur_l + Lr_l Ur_h - (Li_h Ui_h + Li_h Ui_l + Li_l Ui_h)
 //       Im += Lr_h Ui_h + Lr_h Ui_l + Lr_l Ui_h + Li_h Ur_h + Li_h Ur_l + Li_l Ur_h
 //     (the minus via the instruction's negate-A bit; lo*lo is dropped).
-//     Wide form (aosb_factor_set_schur_wide): B tiles are staged as the
-//     N = 384 operand rows [-Ui; Ur; Ui] per hi/lo part, so that one M = 128,
-//     N = 256 MMA takes [Ur | Ui] (rows 128-383) or [-Ui | Ur] (rows 0-255)
-//     and writes both halves [Re | Im] of the accumulator:
-//       [Re|Im] += Lr_h [Ur|Ui]_h + Lr_h [Ur|Ui]_l + Lr_l [Ur|Ui]_h
-//                + Li_h [-Ui|Ur]_h + Li_h [-Ui|Ur]_l + Li_l [-Ui|Ur]_h
-//     -- the same products in the same order per element, six MMAs per slab
-//     instead of twelve, each reading A once for 256 output columns (12 KB
-//     of operands per 128 cycles instead of 8 KB per 64 through the
-//     shared-memory port).
 //     The epilogue writes -acc into 128B-swizzled shared tiles and the TMA
 //     unit adds them into the FP32 target tile in L2
 //     (cp.reduce.async.bulk.tensor .add.f32), so C never passes through
@@ -62,25 +52,6 @@ constexpr int kSlabs = kTcT / kSlabK;     // 8
 constexpr int kPlaneSlabBytes = kTcT * kSlabK * 2;          // 4096
 constexpr int kOperandSlabBytes = 4 * kPlaneSlabBytes;      // 16384
 constexpr int kStagedTileBytes = kSlabs * kOperandSlabBytes;  // 131072
-// Wide B staging: per slab two parts (hi, lo), each two K halves of 384
-// operand rows (-Ui, Ur, Ui) x 16 bytes.
-constexpr int kWideRowBlockBytes = (kTcT / 8) * 128;              // 2048: 128 rows x 16 B
-constexpr int kWideKHalfBytes = 3 * kWideRowBlockBytes;           // 6144
-constexpr int kWidePartBytes = 2 * kWideKHalfBytes;               // 12288
-constexpr int kWideBSlabBytes = 2 * kWidePartBytes;               // 24576
-constexpr int kStagedTileBytesWide = kSlabs * kWideBSlabBytes;    // 196608
-
-__host__ __device__ __forceinline__ int staged_tile_bytes(bool wide) {
-  return wide ? kStagedTileBytesWide : kStagedTileBytes;
-}
-
-// Byte offset of wide B element (n, k) of part (0 hi, 1 lo) in operand row
-// block `which` (0 = -Ui, 1 = Ur, 2 = Ui).
-__host__ __device__ __forceinline__ uint32_t wide_b_offset(int n, int k, int part, int which) {
-  const int slab = k / kSlabK, kk = k % kSlabK;
-  return (uint32_t)(slab * kWideBSlabBytes + part * kWidePartBytes + (kk / 8) * kWideKHalfBytes +
-                    which * kWideRowBlockBytes + (n / 8) * 128 + (n % 8) * 16 + (kk % 8) * 2);
-}
 
 __device__ __forceinline__ size_t tile_base(int64_t p, int64_t n_slots, int64_t slot) {
   return ((size_t)p * (size_t)n_slots + (size_t)slot) * (size_t)(2 * kTcT * kTcT);
@@ -113,7 +84,7 @@ __device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo, __nv_bfloat16 
 }
 
 __device__ __forceinline__ void stage_tile(const float* __restrict__ F, unsigned char* __restrict__ out,
-                                           int kind, const int32_t* __restrict__ pv, bool wide) {
+                                           int kind, const int32_t* __restrict__ pv) {
   const bool a_side = kind == kStageA || kind == kStageAUnitLower;
   // Each thread converts 8 consecutive k of one operand row into one 16-byte
   // chunk of every plane.  Consecutive threads take consecutive operand rows,
@@ -172,21 +143,6 @@ __device__ __forceinline__ void stage_tile(const float* __restrict__ F, unsigned
 #pragma unroll
       for (int pl = 0; pl < 4; ++pl) plane[pl][t / 2] = pack_bf16x2(h[pl][0], h[pl][1]);
     }
-    if (wide && !a_side) {
-      // planes 0-3 = re_hi, re_lo, im_hi, im_lo -> (part, row block); the
-      // negated imaginary planes flip the BF16 sign bits (exact)
-#pragma unroll
-      for (int pl = 0; pl < 4; ++pl) {
-        const int part = pl & 1, which = pl < 2 ? 1 : 2;
-        *reinterpret_cast<uint4*>(out + wide_b_offset(row, k0, part, which)) =
-            make_uint4(plane[pl][0], plane[pl][1], plane[pl][2], plane[pl][3]);
-        if (pl >= 2)
-          *reinterpret_cast<uint4*>(out + wide_b_offset(row, k0, part, 0)) =
-              make_uint4(plane[pl][0] ^ 0x80008000u, plane[pl][1] ^ 0x80008000u,
-                         plane[pl][2] ^ 0x80008000u, plane[pl][3] ^ 0x80008000u);
-      }
-      continue;
-    }
 #pragma unroll
     for (int pl = 0; pl < 4; ++pl)
       *reinterpret_cast<uint4*>(out + staged_offset(row, k0, pl)) =
@@ -206,7 +162,7 @@ __global__ void __launch_bounds__(256) stage_kernel(int nL, int nU, int panel, i
                                                     const float* __restrict__ factor,
                                                     const int32_t* __restrict__ pivots,
                                                     unsigned char* __restrict__ staging,
-                                                    int64_t staging_pencil_stride, bool wide) {
+                                                    int64_t staging_pencil_stride) {
   const int item = blockIdx.x, p = blockIdx.y;
   int slot, kind;
   if (item < nL) {
@@ -221,9 +177,8 @@ __global__ void __launch_bounds__(256) stage_kernel(int nL, int nU, int panel, i
   }
   const float* F = factor + tile_base(p, n_slots, slot);
   const int32_t* pv = pivots + (size_t)p * n_pad + (size_t)k * kTcT;
-  unsigned char* out =
-      staging + (size_t)p * staging_pencil_stride + (size_t)item * staged_tile_bytes(wide);
-  stage_tile(F, out, kind, pv, wide);
+  unsigned char* out = staging + (size_t)p * staging_pencil_stride + (size_t)item * kStagedTileBytes;
+  stage_tile(F, out, kind, pv);
 }
 
 // Persistent, warp-specialized Schur update.  Each CTA (one per SM) walks
@@ -249,10 +204,9 @@ constexpr int kPThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemColsP = 512;
 constexpr int kItemRing = 8;  // > items the producer can run ahead of the epilogue (~4)
 
-template <bool kWide>
 struct PShared {
   alignas(1024) unsigned char a[kStagesP][kOperandSlabBytes];
-  alignas(1024) unsigned char b[kStagesP][kWide ? kWideBSlabBytes : kOperandSlabBytes];
+  alignas(1024) unsigned char b[kStagesP][kOperandSlabBytes];
   uint64_t full[kStagesP];
   uint64_t empty[kStagesP];
   uint64_t acc_full[2];
@@ -367,18 +321,14 @@ __device__ __forceinline__ int item_target(const ItemMap& m, int pair) {
   return m.tslot[a * m.nU + b];
 }
 
-// kWide: B staged in the wide layout, six M = 128, N = 256 MMAs per slab.
-template <bool kWide>
-__global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel_t(
+__global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel(
     const ItemMap map, int n_pencils, int64_t n_slots, const unsigned char* __restrict__ staging,
     const unsigned char* __restrict__ staging1, int64_t staging_pencil_stride,
     int32_t* __restrict__ status, int* __restrict__ claim,
     const __grid_constant__ CUtensorMap tmap_c, long long wl) {
   const int n_pairs = map.n_pairs;
   extern __shared__ unsigned char dyn[];
-  constexpr int kBSlab = kWide ? kWideBSlabBytes : kOperandSlabBytes;
-  constexpr int kTileBytes = kWide ? kStagedTileBytesWide : kStagedTileBytes;
-  PShared<kWide>& sh = *reinterpret_cast<PShared<kWide>*>(
+  PShared& sh = *reinterpret_cast<PShared*>(
       (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int total = n_pairs * n_pencils;
@@ -450,8 +400,8 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel_t(
           if (s == 2 && nxt < total) nnh = item_halves(map, nxt % n_pairs, na, nb, nf);
           const int h = s / kSlabs, sl = s % kSlabs;
           const unsigned char* base = (bf[h] ? staging1 : staging) + (size_t)p * staging_pencil_stride;
-          const unsigned char* stA = base + (size_t)ia[h] * kTileBytes;
-          const unsigned char* stB = base + (size_t)ib[h] * kTileBytes;
+          const unsigned char* stA = base + (size_t)ia[h] * kStagedTileBytes;
+          const unsigned char* stB = base + (size_t)ib[h] * kStagedTileBytes;
           if (!mbar_wait(&sh.empty[stage], phase ^ 1, wl)) {
             sh.failed = 1;
             atomicCAS(&status[p], 0, (int)AOSB_ERR_TIMEOUT);
@@ -459,10 +409,11 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel_t(
           }
           filled |= 1u << stage;
           fill_parity = (fill_parity & ~(1u << stage)) | (phase << stage);
-          mbar_expect_tx(&sh.full[stage], kOperandSlabBytes + kBSlab);
+          mbar_expect_tx(&sh.full[stage], 2 * kOperandSlabBytes);
           bulk_g2s(sh.a[stage], stA + (size_t)sl * kOperandSlabBytes, kOperandSlabBytes,
                    &sh.full[stage]);
-          bulk_g2s(sh.b[stage], stB + (size_t)sl * kBSlab, kBSlab, &sh.full[stage]);
+          bulk_g2s(sh.b[stage], stB + (size_t)sl * kOperandSlabBytes, kOperandSlabBytes,
+                   &sh.full[stage]);
           if (++stage == kStagesP) { stage = 0; phase ^= 1; }
         }
         if (sh.failed) break;
@@ -526,24 +477,6 @@ __global__ void __launch_bounds__(kPThreads, 1) schur_tc_kernel_t(
             Bv[pl] = umma_desc(sb + pl * kPlaneSlabBytes, lbo, sbo);
           }
           const uint32_t first = s == 0 ? 0u : 1u;
-          if constexpr (kWide) {
-            // [Re | Im] += A x [Ur | Ui] (rows 128-383) or A x [-Ui | Ur]
-            // (rows 0-255) per hi/lo part
-            const uint32_t id_w = umma_idesc_mn(kTcT, 2 * kTcT, false);
-            const uint64_t w_h = umma_desc(sb + kWideRowBlockBytes, kWideKHalfBytes, 128);
-            const uint64_t w_l = umma_desc(sb + kWidePartBytes + kWideRowBlockBytes, kWideKHalfBytes, 128);
-            const uint64_t c_h = umma_desc(sb, kWideKHalfBytes, 128);
-            const uint64_t c_l = umma_desc(sb + kWidePartBytes, kWideKHalfBytes, 128);
-            umma_bf16(re, A[0], w_h, id_w, first);
-            umma_bf16(re, A[0], w_l, id_w, 1);
-            umma_bf16(re, A[1], w_h, id_w, 1);
-            umma_bf16(re, A[2], c_h, id_w, 1);
-            umma_bf16(re, A[2], c_l, id_w, 1);
-            umma_bf16(re, A[3], c_h, id_w, 1);
-            umma_commit(&sh.empty[stage]);
-            if (++stage == kStagesP) { stage = 0; phase ^= 1; }
-            continue;
-          }
           umma_bf16(re, A[0], Bv[0], id_pos, first);
           umma_bf16(re, A[0], Bv[1], id_pos, 1);
           umma_bf16(re, A[1], Bv[0], id_pos, 1);
@@ -692,8 +625,7 @@ static int64_t staged_tiles_per_pencil(const aosb_plan* P) {
 constexpr size_t kClaimBytes = 256;
 size_t factor_tc_workspace(const aosb_plan* P, int32_t n_pencils) {
   if (P->T != kTcT) return 0;
-  // sized for the wide B layout whichever form a call uses
-  return 4 * (size_t)staged_tiles_per_pencil(P) * kStagedTileBytesWide * (size_t)n_pencils +
+  return 4 * (size_t)staged_tiles_per_pencil(P) * kStagedTileBytes * (size_t)n_pencils +
          kClaimBytes;
 }
 
@@ -735,11 +667,6 @@ std::atomic<int> g_lookahead_sms{0};
 // process-wide.
 std::atomic<int> g_schur_pairs{0};
 
-// 1: Schur and panel products use the wide B staging and six N = 256 MMAs
-// per slab (ignored while pairs are on, whose loads need the plain
-// layout); process-wide.
-std::atomic<int> g_schur_wide{0};
-
 // Polls of one mbarrier wait before a tensor-core kernel gives up and
 // records AOSB_ERR_TIMEOUT; process-wide, read at each launch.
 std::atomic<long long> g_tc_wait_limit{tc::kTcWaitLimit};
@@ -752,12 +679,8 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     return set_error(err, cap, AOSB_ERR_NULL, "tensor-core path needs a staging workspace");
   cudaStream_t st = (cudaStream_t)a->stream;
   const int np = a->n_pencils;
-  static_assert(sizeof(PShared<false>) + 1024 <= 232448, "shared memory budget");
-  static_assert(sizeof(PShared<true>) + 1024 <= 232448, "shared memory budget (wide)");
-  const bool pairs_on = g_schur_pairs.load() != 0 && P->d_sp_rest != nullptr;
-  const bool wide = g_schur_wide.load() != 0 && !pairs_on;
-  const size_t smem = (wide ? sizeof(PShared<true>) : sizeof(PShared<false>)) + 1024;
-  auto* const schur_tc_kernel = wide ? schur_tc_kernel_t<true> : schur_tc_kernel_t<false>;
+  const size_t smem = sizeof(PShared) + 1024;
+  static_assert(sizeof(PShared) + 1024 <= 232448, "shared memory budget");
   int device = 0, sms = 148;
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -765,19 +688,15 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   static std::atomic<uint64_t> attr_devices{0};
   const uint64_t dev_bit = device < 64 ? (uint64_t)1 << device : 0;
   if (dev_bit == 0 || (attr_devices.load() & dev_bit) == 0) {
-    cudaError_t e = cudaFuncSetAttribute(schur_tc_kernel_t<false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(sizeof(PShared<false>) + 1024));
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(schur_tc_kernel_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(sizeof(PShared<true>) + 1024));
+    cudaError_t e = cudaFuncSetAttribute(schur_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
     if (e != cudaSuccess)
       return set_error(err, cap, AOSB_ERR_CUDA, "schur_tc smem attribute: %s", cudaGetErrorString(e));
     attr_devices.fetch_or(dev_bit);
   }
   // staged tiles per pencil: the step's L and U tiles plus the two
   // diagonal inverses of the panel product
-  const int64_t pencil_stride = staged_tiles_per_pencil(P) * (int64_t)staged_tile_bytes(wide);
+  const int64_t pencil_stride = staged_tiles_per_pencil(P) * (int64_t)kStagedTileBytes;
   unsigned char* staging = (unsigned char*)a->workspace;
   CUtensorMap tmap_c;
   if (int rc = factor_tensor_map(a->factor, (int64_t)np * P->n_slots * 2 * kTcT, &tmap_c, err, cap))
@@ -831,7 +750,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     // L_ik = A_ik inv(U_kk), U_kj = inv(L_kk) P_k A_kj on the tensor cores
     stage_kernel<<<dim3(nL + nU + 2, np), 256, 0, s>>>(
         nL, nU, 1, (int)k, lslot, uslot, P->diag_slot[k], P->n_slots, P->n_pad, a->factor,
-        a->pivots, stage_buf(k), pencil_stride, wide);
+        a->pivots, stage_buf(k), pencil_stride);
     const ItemMap pm{kMapPanel, nL, nU, nL + nU, 0, 0, nullptr, lslot, uslot, nullptr};
     schur_tc_kernel<<<grid_for((int64_t)(nL + nU) * np, cap_ctas), kPThreads, smem, s>>>(
         pm, np, P->n_slots, stage_buf(k), stage_buf(k), pencil_stride, a->status, nullptr, tmap_c, wl);
@@ -846,7 +765,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     stage_kernel<<<dim3(nL + nU, np), 256, 0, s>>>(nL, nU, 0, (int)k, P->d_lb_slot + P->lb_off[k],
                                                   P->d_ur_slot + P->ur_off[k], 0, P->n_slots,
                                                   P->n_pad, a->factor, a->pivots, stage_buf(k),
-                                                  pencil_stride, wide);
+                                                  pencil_stride);
     count_launches(1);
   };
   // Schur update of step k (the pairs `kind` selects) on stream s, untimed
@@ -876,7 +795,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     if (timed)
       timing_end(kTimedSchur, st, ev, (double)items * 8.0 * kTcT * kTcT * kTcT,
                  (double)items * 2.0 * 2 * kTcT * kTcT * sizeof(float) +
-                     (double)(nL + nU) * np * staged_tile_bytes(wide) * ((double)n_pairs / (nL * nU)));
+                     (double)(nL + nU) * np * kStagedTileBytes * ((double)n_pairs / (nL * nU)));
   };
 
   // targets of step k in tile row or column k + 1 (K = 128), on stream s
@@ -893,7 +812,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
   // or the rest items, on stream s (timed); with `claim` the launch takes
   // items from the shared counter instead of a fixed share
   int* claim_counter = reinterpret_cast<int*>(staging + 4 * (int64_t)np * pencil_stride);
-  const bool pairs = pairs_on;
+  const bool pairs = g_schur_pairs.load() != 0 && P->d_sp_rest != nullptr;
   int pair_rc = 0;
   auto two_step = [&](int64_t ss, bool cross, int cap_ctas, cudaStream_t s = nullptr,
                       int* claim = nullptr, bool count_work = true) {
@@ -936,7 +855,7 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
     if (timed)
       timing_end(kTimedSchur, s, ev, halves * np * 8.0 * kTcT * kTcT * kTcT,
                  (double)n * np * 2.0 * 2 * kTcT * kTcT * sizeof(float) +
-                     staged * np * staged_tile_bytes(wide));
+                     staged * np * kStagedTileBytes);
   };
 
   // Two-step (K = 256) updates with lookahead: per super-step (k, k + 1),
@@ -1037,11 +956,6 @@ int factor_tc(const aosb_plan* P, const aosb_factor_args_v1* a, char* err, size_
 }
 
 }  // namespace aosb
-
-extern "C" int32_t aosb_factor_set_schur_wide(int32_t on) {
-  if (on < 0 || on > 1) return -1;
-  return aosb::g_schur_wide.exchange(on);
-}
 
 extern "C" int32_t aosb_factor_set_schur_pairs(int32_t on) {
   if (on < 0 || on > 1) return -1;

@@ -144,7 +144,6 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "aosb_factor_set_lookahead_sms": (c_i32, [c_i32]),
     "aosb_tc_set_wait_limit": (c_i64, [c_i64]),
     "aosb_factor_set_schur_pairs": (c_i32, [c_i32]),
-    "aosb_factor_set_schur_wide": (c_i32, [c_i32]),
     "aosb_solve_set_ctas_per_sm": (c_i32, [c_i32]),
     "aosb_solve_set_lookahead": (c_i32, [c_i32]),
     "aosb_factor": (C.c_int, [c_vp, C.POINTER(FactorArgs), C.c_char_p, c_sz]),

@@ -71,9 +71,6 @@ def parse() -> argparse.Namespace:
                     help="SMs left to the factorization's lookahead side stream (0 = default)")
     ap.add_argument("--schur-pairs", type=int, default=-1, choices=(-1, 0, 1),
                     help="two-CTA (M = 256) pair Schur updates: 1 on, 0 off, -1 library default")
-    ap.add_argument("--schur-wide", type=int, default=-1, choices=(-1, 0, 1),
-                    help="Schur/panel products as N = 256 MMAs on wide-staged U tiles: 1 on, "
-                         "0 off, -1 library default")
     ap.add_argument("--cuda-graphs", type=int, default=-1, choices=(-1, 0, 1),
                     help="replay each batch's triangular sweeps from a CUDA graph: 1 on, 0 off, "
                          "-1 engine default")
@@ -636,10 +633,6 @@ def main() -> None:
         native.library().aosb_factor_set_schur_pairs(args.schur_pairs)
     if args.solve_lookahead >= 0:
         native.library().aosb_solve_set_lookahead(args.solve_lookahead)
-    if args.schur_wide >= 0:
-        native.library().aosb_factor_set_schur_wide(args.schur_wide)
-    wide_on = native.library().aosb_factor_set_schur_wide(0)
-    native.library().aosb_factor_set_schur_wide(wide_on)
     look_on = native.library().aosb_solve_set_lookahead(0)
     native.library().aosb_solve_set_lookahead(look_on)
     pairs_on = native.library().aosb_factor_set_schur_pairs(0)
@@ -808,7 +801,6 @@ def main() -> None:
                    "cuda_graphs": bool(eng.engine.cuda_graphs),
                    "schur_depth": eng.engine.schur_depth,
                    "schur_pairs": bool(pairs_on),
-                   "schur_wide": bool(wide_on) and not bool(pairs_on),
                    "solve_lookahead": bool(look_on),
                    "lookahead_sms": args.lookahead_sms or "default",
                    "solve_ctas_per_sm": args.solve_ctas or "default",

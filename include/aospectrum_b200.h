@@ -333,15 +333,6 @@ int32_t aosb_factor_set_lookahead_sms(int32_t sms);
  * target per CTA.  Process-wide; returns the previous setting (-1 for
  * other values).  No counterpart in the reference. */
 int32_t aosb_factor_set_schur_pairs(int32_t on);
-/* 1: the tensor-core Schur and panel products stage each U tile as the
- * operand rows [-Ui; Ur; Ui] (hi and lo parts) and issue six M = 128,
- * N = 256 MMAs per 16-deep K slab, each writing both the real and the
- * imaginary half of the accumulator, instead of twelve N = 128 MMAs: the
- * same products in the same order per element, with a third fewer operand
- * bytes through the SM's shared-memory port.  0: the N = 128 form.
- * Ignored while two-CTA pairs are on.  Process-wide; returns the previous
- * setting (-1 for other values).  No counterpart in the reference. */
-int32_t aosb_factor_set_schur_wide(int32_t on);
 /* Polls of one mbarrier wait in the tensor-core kernels (factorization
  * Schur/panel products and solve updates) before the waiting CTA gives up:
  * it records AOSB_ERR_TIMEOUT in the pencil's status word, waits (with the

@@ -353,9 +353,6 @@ def test_process_wide_tuning_setters_round_trip():
     prev = lib.aosb_factor_set_schur_pairs(1)
     assert lib.aosb_factor_set_schur_pairs(prev) == 1
     assert lib.aosb_factor_set_schur_pairs(2) == -1
-    prev = lib.aosb_factor_set_schur_wide(1)
-    assert lib.aosb_factor_set_schur_wide(prev) == 1
-    assert lib.aosb_factor_set_schur_wide(-1) == -1
     prev = lib.aosb_tc_set_wait_limit(7)
     assert prev == 1 << 22
     assert lib.aosb_tc_set_wait_limit(0) == 7
