@@ -965,7 +965,7 @@ def fp64_window(pair, interval, dev) -> np.ndarray:
 
 
 def ingest_leg(bundle, dev) -> dict:
-    """Bundle ingest (SURVEY f2) on this box: the bundle is written to a
+    """Bundle ingest on this box: the bundle is written to a
     temporary directory (untimed), then opened memory-mapped (load_bundle),
     its CSR pattern and Bloch tables built by the C++ host code
     (aosb_bloch_create), the block values copied from the memory map into
